@@ -1,0 +1,172 @@
+/*
+ * lumen_gpu.h - device-resident entry points of liblumen (B200, sm_100a).
+ *
+ * These functions take device pointers and a CUDA stream (as void*) and never
+ * see a host copy of the scene. They are what the Python SDK, the torch
+ * autograd function and the render server call through ctypes; lumen.h's
+ * lumen_rasterize is built on them.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   lumen_gpu_render_forward  - rasterize_scene, src/raster/pipeline.mojo:48-52
+ *                               (RenderOutput fields, pipeline.mojo:21-45)
+ *   lumen_gpu_renderer_render - lumen_rasterize, c_api/include/lumen.h:153-159,
+ *                               with library-owned work buffers
+ *   lumen_gpu_render_backward - no counterpart: the reference has no
+ *                               analytic backward (src/optim/gradients.mojo:11-106
+ *                               only stores gradients)
+ *   lumen_gpu_l1_loss         - compute_l1_loss, src/optim/loss.mojo:11-35
+ *   lumen_gpu_sort_pairs      - radix_sort_64bit, src/raster/radix_sort.mojo:39-87
+ *
+ * Threading: no global state; every call works only on the buffers it is
+ * given and enqueues on the given stream. Functions that wait say so.
+ * Limits: instance counts below 2^30, Gaussian counts below 2^31.
+ */
+#ifndef LUMEN_GPU_H
+#define LUMEN_GPU_H
+
+#include "lumen.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Gaussians in device memory, float32, contiguous SoA:
+ * means [N,3], scales [N,3] (linear, or log-scales when params_are_logits),
+ * quats [N,4] (w,x,y,z, any norm), opacities [N] ([0,1], or logits),
+ * sh [N,16,3] (sh[i*48 + coef*3 + ch]). */
+typedef struct {
+    const float* means;
+    const float* scales;
+    const float* quats;
+    const float* opacities;
+    const float* sh;
+    int64_t count;
+} LumenGpuGaussians;
+
+/* Pinhole camera in the reference PinholeCamera convention
+ * (src/scene/camera.mojo:24-79): camera-space point = rotation^-1 (p - position),
+ * identity looks down +z, image x right and y down. */
+typedef struct {
+    float position[3];
+    float rotation[4];              /* w, x, y, z; normalised by the kernels */
+    float fx, fy, cx, cy;
+    float near_plane, far_plane;
+    int32_t width, height;
+} LumenViewCamera;
+
+/* RenderConfig fields read on the path (src/core/config.mojo:65-102) plus:
+ * key_mode 0 = millimetre depth key (radix_sort.mojo:8-18), 1 = float bits;
+ * term_mode 0 = stop a pixel when T <= term_threshold (1e-4, compositor.mojo:53),
+ *           1 = stop when 1 - T >= term_threshold (0.99);
+ * params_are_logits 1 = scales are log-scales, opacities are logits. */
+typedef struct {
+    float lowpass;
+    int32_t sh_degree;
+    int32_t white_background;
+    int32_t compute_depth;
+    int32_t key_mode;
+    int32_t term_mode;
+    int32_t params_are_logits;
+    int32_t tile_size;              /* must be 16 */
+    float term_threshold;
+} LumenRenderOptions;
+
+/* One projected splat (pipeline.mojo:141-149), 48 bytes, indexed by the
+ * compacted visible index. ic* is Covariance2D.inverse(). */
+typedef struct {
+    float cx, cy, depth, opacity;
+    float ic00, ic01, ic11, pad0;
+    float r, g, b, pad1;
+} LumenSplatRecord;
+
+/* Work buffers of one frame, device memory owned by the caller.
+ * records/visible_ids/radii hold n_gaussians entries; keys/vals hold
+ * instance_capacity entries each (two ping-pong sets); ranges holds
+ * 2 * n_tiles int32 (start, end; -1,-1 for an empty tile, as
+ * binning.mojo:10-28); scratch is lumen_gpu_scratch_bytes() bytes. */
+typedef struct {
+    LumenSplatRecord* records;
+    uint32_t* visible_ids;
+    int32_t* radii;
+    uint64_t* keys[2];
+    uint32_t* vals[2];
+    int64_t instance_capacity;
+    int32_t* ranges;
+    void* scratch;
+    size_t scratch_bytes;
+} LumenGpuFrame;
+
+/* Per-pixel outputs in device memory. rgb [H,W,3] is required; the others
+ * may be NULL. depth [H,W] alpha-weighted depth; alpha [H,W] = 1 - T;
+ * n_contrib [H,W] splats blended (the terminating one included);
+ * last_idx [H,W] sorted index of the last instance visited, -1 if none. */
+typedef struct {
+    float* rgb;
+    float* depth;
+    float* alpha;
+    uint32_t* n_contrib;
+    int32_t* last_idx;
+} LumenGpuImage;
+
+/* Frame counters read back by lumen_gpu_read_counts. error_flags bits:
+ * 1 = instances exceeded instance_capacity (outputs invalid; re-run with a
+ *     larger frame), 2 = a bounded spin-wait gave up (outputs invalid),
+ * 4 = invalid launch parameters. sorted_buffer: which of keys[0]/keys[1]
+ * holds the sorted keys. varying_digits: bit d set when byte d of the keys
+ * varies (only those digit passes run). */
+typedef struct {
+    int64_t n_visible;
+    int64_t n_instances;
+    uint32_t error_flags;
+    uint32_t sorted_buffer;
+    uint32_t varying_digits;
+    uint32_t touched_tiles;
+} LumenGpuCounts;
+
+#define LUMEN_GPU_ERR_CAPACITY 1u
+#define LUMEN_GPU_ERR_SPIN_TIMEOUT 2u
+#define LUMEN_GPU_ERR_LAUNCH 4u
+
+/* Bytes of scratch a frame needs (control block, look-back descriptors,
+ * digit histograms). */
+size_t lumen_gpu_scratch_bytes(int64_t n_gaussians, int64_t instance_capacity, int64_t n_tiles);
+
+/* Enqueue the whole forward on `stream`: project + cull + SH + compacting
+ * scan + key emit, histogram, stable LSD digit passes, tile ranges,
+ * compositing. Does not wait. */
+LumenStatus lumen_gpu_render_forward(const LumenGpuGaussians* gaussians, const LumenViewCamera* camera,
+                                     const LumenRenderOptions* options, LumenGpuFrame* frame,
+                                     LumenGpuImage* image, void* stream);
+
+/* Wait for `stream`, then read the frame counters. */
+LumenStatus lumen_gpu_read_counts(const LumenGpuFrame* frame, LumenGpuCounts* counts, void* stream);
+
+/* A renderer owns its work buffers and grows them on demand. */
+typedef struct LumenGpuRenderer LumenGpuRenderer;
+LumenGpuRenderer* lumen_gpu_renderer_create(void);
+void lumen_gpu_renderer_destroy(LumenGpuRenderer* renderer);
+/* Render and wait; re-runs once with larger buffers if the instance count
+ * exceeded the current capacity. */
+LumenStatus lumen_gpu_renderer_render(LumenGpuRenderer* renderer, const LumenGpuGaussians* gaussians,
+                                      const LumenViewCamera* camera, const LumenRenderOptions* options,
+                                      LumenGpuImage* image, LumenGpuCounts* counts, void* stream);
+/* The renderer's frame (valid after a render; for inspection and backward). */
+const LumenGpuFrame* lumen_gpu_renderer_frame(const LumenGpuRenderer* renderer);
+
+/* Stable sort of n (key, value) pairs by key, in place in keys[0]/vals[0]
+ * with keys[1]/vals[1] as the alternate buffers; the sorted data ends in the
+ * set named by *sorted_buffer (device-side digit skipping decides). The
+ * scratch must hold lumen_gpu_scratch_bytes(0, n, 0) bytes. Waits. */
+LumenStatus lumen_gpu_sort_pairs(uint64_t* keys0, uint32_t* vals0, uint64_t* keys1, uint32_t* vals1,
+                                 int64_t n, void* scratch, size_t scratch_bytes, uint32_t* sorted_buffer,
+                                 void* stream);
+
+/* Append n splats to a cloud in one copy. No counterpart in the reference:
+ * the bulk form of lumen_cloud_add_gaussian (c_api/include/lumen.h:129),
+ * with the same growth rule and error codes. */
+LumenStatus lumen_cloud_append(LumenCloud* cloud, const LumenGaussian* gaussians, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUMEN_GPU_H */

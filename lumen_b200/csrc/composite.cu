@@ -1,0 +1,126 @@
+/*
+ * composite.cu - K5: per-tile front-to-back alpha compositing.
+ *
+ * Reference: the per-tile pixel loop of rasterize_scene,
+ * src/raster/pipeline.mojo:172-229, with compute_gaussian_pixel_alpha and
+ * PixelAccumulator.blend/finalize, src/raster/compositor.mojo:10-89.
+ *
+ * One CTA per 16x16 tile, one thread per pixel. The tile's sorted instances
+ * are processed in chunks of 256: each thread gathers one instance's
+ * 48-byte record (through the sorted visible index) into shared memory,
+ * then every thread walks the chunk in order, so each pixel blends its
+ * splats in exactly the reference order. A pixel stops after the blend that
+ * saturates it; a warp leaves the chunk once all its pixels stopped, and the
+ * CTA stops loading chunks once all 256 pixels stopped.
+ *
+ * Built with --fmad=false: power, alpha, weights and transmittance round as
+ * in the reference, so contributor counts match the CPU restatement bit for
+ * bit. The exponential is lumen_expf (shared with the restatement).
+ */
+#include "splat_common.cuh"
+
+namespace lumen {
+
+struct CompositeSmem {
+    float4 geo[kTilePixels];   /* cx, cy, depth, opacity */
+    float4 con[kTilePixels];   /* ic00, ic01, ic11, - */
+    float4 col[kTilePixels];   /* r, g, b, - */
+};
+
+__global__ void __launch_bounds__(kTilePixels)
+composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, long long capacity,
+                 const Control* __restrict__ ctrl, int width, int height, int tiles_x,
+                 LumenRenderOptions opt, LumenGpuImage img) {
+    __shared__ CompositeSmem s;
+    const int tile = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    const int px = tx * kTile + (tid & 15), py = ty * kTile + (tid >> 4);
+    const bool inside = px < width && py < height;
+    const long long pix = (long long)py * width + px;
+    const long long K = (long long)ctrl->n_instances < capacity ? (long long)ctrl->n_instances : capacity;
+
+    float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, dep = 0.0f, acc = 0.0f;
+    unsigned int count = 0;
+    int last = -1;
+    bool background = opt.white_background != 0;
+
+    if (K == 0) {
+        /* pipeline.mojo:162-163: no instances, the output stays zero */
+        background = false;
+    } else {
+        const int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
+        if (!(rs == -1 || rs >= re)) {
+            const unsigned int* __restrict__ vals = ctrl->sorted_buffer ? f.vals[1] : f.vals[0];
+            const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+            const float thr = opt.term_threshold;
+            const bool mode_alpha = opt.term_mode == 1;
+            bool done = !inside;
+            for (int cs = rs; cs < re; cs += kTilePixels) {
+                if (__syncthreads_count(!done) == 0) break;
+                const int i = cs + tid;
+                if (i < re) {
+                    const float4* r4 = reinterpret_cast<const float4*>(records + vals[i]);
+                    s.geo[tid] = __ldg(r4);
+                    s.con[tid] = __ldg(r4 + 1);
+                    s.col[tid] = __ldg(r4 + 2);
+                }
+                __syncthreads();
+                const int n = re - cs < kTilePixels ? re - cs : kTilePixels;
+                for (int j = 0; j < n; ++j) {
+                    if (!done) {
+                        last = cs + j;
+                        const float4 gg = s.geo[j];
+                        const float4 cc = s.con[j];
+                        /* compute_gaussian_pixel_alpha, compositor.mojo:62-89 */
+                        const float dx = pxc - gg.x;
+                        const float dy = pyc - gg.y;
+                        float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
+                        bool skip = false;
+                        if (power < 0.0f) power = 0.0f;
+                        else if (power > 4.5f) skip = true;
+                        if (!skip) {
+                            float alpha = gg.w * lumen_expf(-power);
+                            if (alpha > (float)0.99) alpha = (float)0.99;
+                            /* PixelAccumulator.blend, compositor.mojo:25-53 */
+                            if (!(alpha < min_alpha())) {
+                                const float4 col = s.col[j];
+                                const float w = alpha * T;
+                                cr += col.x * w;
+                                cg += col.y * w;
+                                cb += col.z * w;
+                                dep += gg.z * w;
+                                T *= (1.0f - alpha);
+                                acc = 1.0f - T;
+                                ++count;
+                                if (mode_alpha ? (acc >= thr) : (T <= thr)) done = true;
+                            }
+                        }
+                    }
+                    if (__all_sync(0xffffffffu, done)) break;
+                }
+                __syncthreads();
+            }
+        }
+    }
+    if (!inside) return;
+    /* finalize, compositor.mojo:55-59 */
+    if (background) { cr += T; cg += T; cb += T; }
+    img.rgb[pix * 3 + 0] = cr;
+    img.rgb[pix * 3 + 1] = cg;
+    img.rgb[pix * 3 + 2] = cb;
+    if (img.depth) img.depth[pix] = opt.compute_depth ? dep : 0.0f;
+    if (img.alpha) img.alpha[pix] = acc;
+    if (img.n_contrib) img.n_contrib[pix] = count;
+    if (img.last_idx) img.last_idx[pix] = last;
+}
+
+void launch_composite(const LumenGpuFrame& f, const Control* ctrl, const LumenViewCamera& cam,
+                      const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st) {
+    const int tiles_x = (cam.width + kTile - 1) / kTile;
+    const int tiles_y = (cam.height + kTile - 1) / kTile;
+    composite_kernel<<<tiles_x * tiles_y, kTilePixels, 0, st>>>(
+        f.records, f, (long long)f.instance_capacity, ctrl, cam.width, cam.height, tiles_x, opt, img);
+}
+
+}  // namespace lumen

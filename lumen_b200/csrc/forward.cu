@@ -1,0 +1,290 @@
+/*
+ * forward.cu - host side of the device API declared in include/lumen_gpu.h:
+ * argument checks, scratch layout, the launch sequence of one frame, and a
+ * renderer that owns and grows its frame buffers.
+ *
+ * Launch sequence of a frame (all on the caller's stream, no host sync):
+ *   memset(control + project look-back)
+ *   project_emit      K1 (projection, compacting scan, key emission)
+ *   sort_histogram    digit histograms; clears look-back; ranges = -1
+ *   onesweep_pass x8  K3 (a pass whose digit is constant exits at once)
+ *   tile_ranges       K4
+ *   composite         K5
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "splat_common.cuh"
+
+namespace lumen {
+void launch_project_emit(const LumenGpuGaussians& g, const LumenViewCamera& cam, const LumenRenderOptions& opt,
+                         LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, cudaStream_t st);
+void launch_sort(LumenGpuFrame& f, Control* ctrl, unsigned int* sort_lb, long long lb_tiles_cap,
+                 long long n_range_ints, int num_sms, cudaStream_t st);
+void launch_ranges(LumenGpuFrame& f, Control* ctrl, int num_sms, cudaStream_t st);
+void launch_key_stats(const unsigned long long* keys, long long n, Control* ctrl, int num_sms, cudaStream_t st);
+void launch_composite(const LumenGpuFrame& f, const Control* ctrl, const LumenViewCamera& cam,
+                      const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st);
+void configure_sort_kernels();
+
+int device_sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 148;
+    return n;
+}
+
+static void configure_once() {
+    static std::once_flag once;
+    std::call_once(once, [] { configure_sort_kernels(); });
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt) {
+    if (!g || !cam || !opt) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (g->count < 0 || g->count >= (1ll << 31)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (g->count > 0) {
+        if (!g->means || !g->scales || !g->quats || !g->opacities || !g->sh) return LUMEN_ERROR_INVALID_ARGUMENT;
+        if (!aligned16(g->quats) || !aligned16(g->sh)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    }
+    if (cam->width <= 0 || cam->height <= 0 || cam->width > 65535 * kTile || cam->height > 65535 * kTile)
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (opt->tile_size != kTile) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (opt->sh_degree < 0 || opt->sh_degree > 3) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (opt->key_mode < 0 || opt->key_mode > 1 || opt->term_mode < 0 || opt->term_mode > 1)
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    return LUMEN_SUCCESS;
+}
+
+/* Device-side failures: capacity still exceeded -> out of memory; a bounded
+ * wait that gave up or a bad launch -> I/O failure (the device did not
+ * complete the frame). */
+static LumenStatus status_from_flags(unsigned int flags) {
+    if (flags & LUMEN_GPU_ERR_CAPACITY) return LUMEN_ERROR_OUT_OF_MEMORY;
+    if (flags) return LUMEN_ERROR_IO_FAILURE;
+    return LUMEN_SUCCESS;
+}
+
+static LumenGpuFrame f_scratch_only(void* scratch, size_t bytes) {
+    LumenGpuFrame f;
+    std::memset(&f, 0, sizeof(f));
+    f.scratch = scratch;
+    f.scratch_bytes = bytes;
+    return f;
+}
+
+static LumenStatus map_cuda(cudaError_t e) {
+    if (e == cudaSuccess) return LUMEN_SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return LUMEN_ERROR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInitializationError)
+        return LUMEN_ERROR_UNINITIALIZED;
+    return LUMEN_ERROR_INVALID_ARGUMENT;
+}
+
+}  // namespace lumen
+
+using namespace lumen;
+
+extern "C" {
+
+size_t lumen_gpu_scratch_bytes(int64_t n_gaussians, int64_t instance_capacity, int64_t n_tiles) {
+    (void)n_tiles;
+    return ScratchLayout::make(n_gaussians, instance_capacity).total;
+}
+
+LumenStatus lumen_gpu_render_forward(const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                     const LumenRenderOptions* opt, LumenGpuFrame* f, LumenGpuImage* img,
+                                     void* stream) {
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    if (!f || !img || !img->rgb || !f->scratch || !f->ranges || f->instance_capacity <= 0 ||
+        f->instance_capacity >= (1ll << 30) || !f->keys[0] || !f->keys[1] || !f->vals[0] || !f->vals[1])
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (g->count > 0 && (!f->records || !f->visible_ids || !f->radii)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    const ScratchLayout L = ScratchLayout::make(g->count, f->instance_capacity);
+    if (f->scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
+    configure_once();
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* base = (unsigned char*)f->scratch;
+    Control* ctrl = (Control*)(base + L.control_off);
+    unsigned long long* plb = (unsigned long long*)(base + L.proj_lb_off);
+    unsigned int* slb = (unsigned int*)(base + L.sort_lb_off);
+    cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (g->count > 0) launch_project_emit(*g, *cam, *opt, *f, ctrl, plb, (int)L.proj_blocks, s);
+    const long long tiles = (long long)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
+    const int sms = device_sm_count();
+    launch_sort(*f, ctrl, slb, L.sort_tiles, 2 * tiles, sms, s);
+    launch_ranges(*f, ctrl, sms, s);
+    launch_composite(*f, ctrl, *cam, *opt, *img, s);
+    e = cudaGetLastError();
+    return map_cuda(e);
+}
+
+LumenStatus lumen_gpu_read_counts(const LumenGpuFrame* f, LumenGpuCounts* c, void* stream) {
+    if (!f || !c || !f->scratch) return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    Control h;
+    cudaError_t e = cudaMemcpyAsync(&h, f->scratch, offsetof(Control, hist), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return map_cuda(e);
+    c->n_visible = h.n_visible;
+    c->n_instances = (int64_t)h.n_instances;
+    c->error_flags = h.error_flags;
+    c->sorted_buffer = h.sorted_buffer;
+    c->varying_digits = h.varying_digits;
+    c->touched_tiles = h.touched_tiles;
+    return LUMEN_SUCCESS;
+}
+
+}  // extern "C"
+
+/* ---------------------------------------------------------------- renderer */
+
+struct LumenGpuRenderer {
+    LumenGpuFrame frame;
+    int64_t n_cap = 0;       /* Gaussians the per-Gaussian buffers hold */
+    int64_t tiles_cap = 0;
+    int64_t k_cap = 0;
+    int device = -1;
+};
+
+namespace {
+
+void free_frame(LumenGpuRenderer* r) {
+    LumenGpuFrame& f = r->frame;
+    cudaFree(f.records); cudaFree(f.visible_ids); cudaFree(f.radii);
+    cudaFree(f.keys[0]); cudaFree(f.keys[1]); cudaFree(f.vals[0]); cudaFree(f.vals[1]);
+    cudaFree(f.ranges); cudaFree(f.scratch);
+    std::memset(&f, 0, sizeof(f));
+    r->n_cap = r->tiles_cap = r->k_cap = 0;
+}
+
+/* Grow the buffers to hold n Gaussians, `tiles` tiles and k instances. */
+LumenStatus ensure(LumenGpuRenderer* r, int64_t n, int64_t tiles, int64_t k) {
+    LumenGpuFrame& f = r->frame;
+    cudaError_t e = cudaSuccess;
+    if (n > r->n_cap) {
+        int64_t nn = n + n / 8 + 1024;
+        cudaFree(f.records); cudaFree(f.visible_ids); cudaFree(f.radii);
+        f.records = nullptr; f.visible_ids = nullptr; f.radii = nullptr;
+        r->n_cap = 0;
+        if ((e = cudaMalloc(&f.records, nn * sizeof(LumenSplatRecord))) != cudaSuccess) return map_cuda(e);
+        if ((e = cudaMalloc(&f.visible_ids, nn * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
+        if ((e = cudaMalloc(&f.radii, nn * sizeof(int32_t))) != cudaSuccess) return map_cuda(e);
+        r->n_cap = nn;
+    }
+    if (tiles > r->tiles_cap) {
+        cudaFree(f.ranges);
+        f.ranges = nullptr;
+        r->tiles_cap = 0;
+        if ((e = cudaMalloc(&f.ranges, tiles * 2 * sizeof(int32_t))) != cudaSuccess) return map_cuda(e);
+        r->tiles_cap = tiles;
+    }
+    if (k > r->k_cap) {
+        int64_t kk = k + k / 4 + 4096;
+        if (kk >= (1ll << 30)) kk = (1ll << 30) - 1;
+        if (k > kk) return LUMEN_ERROR_OUT_OF_MEMORY;
+        for (int b = 0; b < 2; ++b) {
+            cudaFree(f.keys[b]); cudaFree(f.vals[b]);
+            f.keys[b] = nullptr; f.vals[b] = nullptr;
+        }
+        r->k_cap = 0;
+        f.instance_capacity = 0;
+        for (int b = 0; b < 2; ++b) {
+            if ((e = cudaMalloc(&f.keys[b], kk * sizeof(uint64_t))) != cudaSuccess) return map_cuda(e);
+            if ((e = cudaMalloc(&f.vals[b], kk * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
+        }
+        r->k_cap = kk;
+        f.instance_capacity = kk;
+    }
+    const size_t need = ScratchLayout::make(r->n_cap, r->k_cap).total;
+    if (need > f.scratch_bytes) {
+        cudaFree(f.scratch);
+        f.scratch = nullptr;
+        f.scratch_bytes = 0;
+        if ((e = cudaMalloc(&f.scratch, need)) != cudaSuccess) return map_cuda(e);
+        f.scratch_bytes = need;
+    }
+    return LUMEN_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+LumenGpuRenderer* lumen_gpu_renderer_create(void) {
+    LumenGpuRenderer* r = new (std::nothrow) LumenGpuRenderer();
+    if (!r) return nullptr;
+    std::memset(&r->frame, 0, sizeof(r->frame));
+    if (cudaGetDevice(&r->device) != cudaSuccess) { delete r; return nullptr; }
+    return r;
+}
+
+void lumen_gpu_renderer_destroy(LumenGpuRenderer* r) {
+    if (!r) return;
+    free_frame(r);
+    delete r;
+}
+
+const LumenGpuFrame* lumen_gpu_renderer_frame(const LumenGpuRenderer* r) { return r ? &r->frame : nullptr; }
+
+LumenStatus lumen_gpu_renderer_render(LumenGpuRenderer* r, const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                      const LumenRenderOptions* opt, LumenGpuImage* img, LumenGpuCounts* counts,
+                                      void* stream) {
+    if (!r) return LUMEN_ERROR_INVALID_ARGUMENT;
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    const int64_t tiles = (int64_t)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
+    int64_t k_guess = r->k_cap > 0 ? r->k_cap : (g->count * 8 > (1 << 20) ? g->count * 8 : (1 << 20));
+    st = ensure(r, g->count > 0 ? g->count : 1, tiles, k_guess);
+    if (st != LUMEN_SUCCESS) return st;
+    LumenGpuCounts c;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        st = lumen_gpu_render_forward(g, cam, opt, &r->frame, img, stream);
+        if (st != LUMEN_SUCCESS) return st;
+        st = lumen_gpu_read_counts(&r->frame, &c, stream);
+        if (st != LUMEN_SUCCESS) return st;
+        if (!(c.error_flags & LUMEN_GPU_ERR_CAPACITY)) break;
+        st = ensure(r, g->count, tiles, c.n_instances);
+        if (st != LUMEN_SUCCESS) return st;
+    }
+    if (counts) *counts = c;
+    return status_from_flags(c.error_flags);
+}
+
+LumenStatus lumen_gpu_sort_pairs(uint64_t* keys0, uint32_t* vals0, uint64_t* keys1, uint32_t* vals1, int64_t n,
+                                 void* scratch, size_t scratch_bytes, uint32_t* sorted_buffer, void* stream) {
+    if (n < 0 || n >= (1ll << 30) || !sorted_buffer) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (n > 0 && (!keys0 || !vals0 || !keys1 || !vals1 || !scratch)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    *sorted_buffer = 0;
+    if (n == 0) return LUMEN_SUCCESS;
+    const ScratchLayout L = ScratchLayout::make(0, n);
+    if (scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
+    configure_once();
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* base = (unsigned char*)scratch;
+    Control* ctrl = (Control*)(base + L.control_off);
+    cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
+    if (e != cudaSuccess) return map_cuda(e);
+    LumenGpuFrame f;
+    std::memset(&f, 0, sizeof(f));
+    f.keys[0] = keys0; f.keys[1] = keys1; f.vals[0] = vals0; f.vals[1] = vals1;
+    f.instance_capacity = n;
+    const int sms = device_sm_count();
+    launch_key_stats(reinterpret_cast<const unsigned long long*>(keys0), n, ctrl, sms, s);
+    launch_sort(f, ctrl, (unsigned int*)(base + L.sort_lb_off), L.sort_tiles, 0, sms, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return map_cuda(e);
+    LumenGpuCounts c;
+    const LumenGpuFrame fs = f_scratch_only(scratch, scratch_bytes);
+    LumenStatus st = lumen_gpu_read_counts(&fs, &c, stream);
+    if (st != LUMEN_SUCCESS) return st;
+    *sorted_buffer = c.sorted_buffer;
+    return status_from_flags(c.error_flags);
+}
+
+}  // extern "C"

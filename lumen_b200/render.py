@@ -1,0 +1,178 @@
+"""Device-resident forward render through the C ABI (lumen_gpu_render_forward).
+
+PyTorch supplies device memory and the current CUDA stream; all computation
+is in liblumen.so. This is the Python form of the reference's
+``rasterize_scene(cloud, camera, config) -> RenderOutput``
+(src/raster/pipeline.mojo:48-52): it returns the image, depth, alpha, the
+per-pixel contributor counts and every intermediate stage (records, sorted
+keys and values, tile ranges) for inspection.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+
+from . import _lib as L
+from .types import RenderOptions, ViewCamera
+
+RECORD_FLOATS = 12
+
+
+def _p(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+@dataclass
+class Frame:
+    """Work buffers of one frame (torch-owned device memory)."""
+    records: torch.Tensor       # [N, 12] float32 (48-byte records by visible index)
+    visible_ids: torch.Tensor   # [N] int32 (Gaussian index of each record)
+    radii: torch.Tensor         # [N] int32
+    keys: list                  # 2 x [cap] int64 (uint64 bits)
+    vals: list                  # 2 x [cap] int32 (uint32 bits)
+    ranges: torch.Tensor        # [tiles, 2] int32
+    scratch: torch.Tensor       # uint8
+    capacity: int
+
+    @staticmethod
+    def allocate(n: int, tiles: int, capacity: int, device) -> "Frame":
+        lib = L.load()
+        n1 = max(n, 1)
+        scratch_bytes = int(lib.lumen_gpu_scratch_bytes(n1, capacity, tiles))
+        kw = dict(device=device)
+        return Frame(torch.empty((n1, RECORD_FLOATS), dtype=torch.float32, **kw),
+                     torch.empty(n1, dtype=torch.int32, **kw), torch.empty(n1, dtype=torch.int32, **kw),
+                     [torch.empty(capacity, dtype=torch.int64, **kw) for _ in range(2)],
+                     [torch.empty(capacity, dtype=torch.int32, **kw) for _ in range(2)],
+                     torch.empty((tiles, 2), dtype=torch.int32, **kw),
+                     torch.empty(scratch_bytes, dtype=torch.uint8, **kw), capacity)
+
+    def fits(self, n: int, tiles: int) -> bool:
+        return self.records.shape[0] >= max(n, 1) and self.ranges.shape[0] >= tiles
+
+    def c_struct(self) -> L.LumenGpuFrame:
+        f = L.LumenGpuFrame()
+        f.records, f.visible_ids, f.radii = _p(self.records), _p(self.visible_ids), _p(self.radii)
+        f.keys[0], f.keys[1] = _p(self.keys[0]), _p(self.keys[1])
+        f.vals[0], f.vals[1] = _p(self.vals[0]), _p(self.vals[1])
+        f.instance_capacity = self.capacity
+        f.ranges = _p(self.ranges)
+        f.scratch = _p(self.scratch)
+        f.scratch_bytes = self.scratch.numel()
+        return f
+
+
+@dataclass
+class RenderResult:
+    rgb: torch.Tensor            # [H, W, 3]
+    depth: torch.Tensor          # [H, W]
+    alpha: torch.Tensor          # [H, W] 1 - T
+    n_contrib: torch.Tensor      # [H, W] int32
+    last_idx: torch.Tensor       # [H, W] int32
+    n_visible: int
+    n_instances: int
+    touched_tiles: int
+    varying_digits: int
+    sorted_buffer: int
+    frame: Frame
+
+    @property
+    def sorted_keys(self) -> torch.Tensor:
+        return self.frame.keys[self.sorted_buffer][: self.n_instances]
+
+    @property
+    def sorted_vals(self) -> torch.Tensor:
+        return self.frame.vals[self.sorted_buffer][: self.n_instances]
+
+    @property
+    def records(self) -> torch.Tensor:
+        return self.frame.records[: self.n_visible]
+
+    @property
+    def ranges(self) -> torch.Tensor:
+        return self.frame.ranges
+
+
+def gaussians_struct(means, scales, quats, opacities, sh) -> L.LumenGpuGaussians:
+    n = int(means.shape[0])
+    for name, t, shape in (("means", means, (n, 3)), ("scales", scales, (n, 3)), ("quats", quats, (n, 4)),
+                           ("opacities", opacities, (n,)), ("sh", sh, (n, 48))):
+        if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous float32 CUDA tensor")
+        if tuple(t.reshape(shape).shape) != shape:
+            raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {shape}")
+    g = L.LumenGpuGaussians()
+    g.means, g.scales, g.quats, g.opacities, g.sh = _p(means), _p(scales), _p(quats), _p(opacities), _p(sh)
+    g.count = n
+    return g
+
+
+_capacity_hint = {}
+
+
+def render(means: torch.Tensor, scales: torch.Tensor, quats: torch.Tensor, opacities: torch.Tensor,
+           sh: torch.Tensor, camera: ViewCamera, options: Optional[RenderOptions] = None,
+           frame: Optional[Frame] = None, capacity: Optional[int] = None) -> RenderResult:
+    """Forward render on the tensors' device. ``scales``/``opacities`` are linear
+    and in [0, 1] unless ``options.params_are_logits``. Waits for the frame to
+    finish (it reads the instance count back to check the buffer capacity)."""
+    options = options or RenderOptions()
+    lib = L.load()
+    dev = means.device
+    n = int(means.shape[0])
+    H, W = int(camera.height), int(camera.width)
+    tiles = camera.n_tiles
+    g = gaussians_struct(means, scales, quats, opacities, sh.reshape(n, 48) if n else sh.reshape(0, 48))
+    cam, opt = L.view_camera(camera), L.render_options(options)
+    rgb = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+    depth = torch.empty((H, W), dtype=torch.float32, device=dev)
+    alpha = torch.empty((H, W), dtype=torch.float32, device=dev)
+    ncon = torch.empty((H, W), dtype=torch.int32, device=dev)
+    last = torch.empty((H, W), dtype=torch.int32, device=dev)
+    img = L.LumenGpuImage()
+    img.rgb, img.depth, img.alpha, img.n_contrib, img.last_idx = _p(rgb), _p(depth), _p(alpha), _p(ncon), _p(last)
+    key = (n, W, H)
+    if capacity is None:
+        capacity = _capacity_hint.get(key, max(1 << 16, 8 * n))
+    if frame is None or not frame.fits(n, tiles) or frame.capacity < capacity:
+        frame = Frame.allocate(n, tiles, capacity, dev)
+    stream = _stream_handle(dev)
+    counts = L.LumenGpuCounts()
+    for _ in range(2):
+        fs = frame.c_struct()
+        L.check(lib.lumen_gpu_render_forward(C.byref(g), C.byref(cam), C.byref(opt), C.byref(fs), C.byref(img),
+                                             stream), "render_forward")
+        L.check(lib.lumen_gpu_read_counts(C.byref(fs), C.byref(counts), stream), "read_counts")
+        if not counts.error_flags & L.ERR_CAPACITY:
+            break
+        need = int(counts.n_instances)
+        capacity = need + need // 4 + 4096
+        frame = Frame.allocate(n, tiles, capacity, dev)
+    if counts.error_flags:
+        raise L.LumenError(-4 if not counts.error_flags & L.ERR_CAPACITY else -2,
+                           f"render_forward device flags {counts.error_flags:#x}")
+    _capacity_hint[key] = frame.capacity
+    return RenderResult(rgb, depth, alpha, ncon, last, int(counts.n_visible), int(counts.n_instances),
+                        int(counts.touched_tiles), int(counts.varying_digits), int(counts.sorted_buffer), frame)
+
+
+def sort_pairs(keys: torch.Tensor, vals: torch.Tensor):
+    """Stable sort of (uint64 key, uint32 value) pairs on the device
+    (lumen_gpu_sort_pairs). Takes int64/int32 tensors holding the bits;
+    returns sorted copies."""
+    lib = L.load()
+    n = int(keys.numel())
+    k0, v0 = keys.contiguous().clone(), vals.contiguous().clone()
+    k1, v1 = torch.empty_like(k0), torch.empty_like(v0)
+    scratch = torch.empty(int(lib.lumen_gpu_scratch_bytes(0, max(n, 1), 0)), dtype=torch.uint8, device=keys.device)
+    sb = C.c_uint32(0)
+    L.check(lib.lumen_gpu_sort_pairs(_p(k0), _p(v0), _p(k1), _p(v1), n, _p(scratch), scratch.numel(), C.byref(sb),
+                                     _stream_handle(keys.device)), "sort_pairs")
+    return (k1, v1) if sb.value else (k0, v0)

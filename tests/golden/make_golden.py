@@ -1,0 +1,50 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+capi_synthetic.npz: the splats the reference C library
+(c_api/src/lumen_c.c:156-256, built into oracle/_ref/liblumen_ref.so by
+``make -C oracle ref``) generates for lumen_create_synthetic_cube(4, 2.0) and
+lumen_create_synthetic_sphere(128, 1.5), as [n, 59] float32 rows in
+LumenGaussian field order. The reference source is needed only to run this
+script; the tests read the committed .npz.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.path.join(ROOT, "oracle", "_ref", "liblumen_ref.so")
+
+
+def main():
+    if not os.path.exists(REF):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    lib = C.CDLL(REF)
+    lib.lumen_create_synthetic_cube.restype = C.c_void_p
+    lib.lumen_create_synthetic_cube.argtypes = [C.c_size_t, C.c_float]
+    lib.lumen_create_synthetic_sphere.restype = C.c_void_p
+    lib.lumen_create_synthetic_sphere.argtypes = [C.c_size_t, C.c_float]
+    lib.lumen_cloud_get_count.restype = C.c_size_t
+    lib.lumen_cloud_get_count.argtypes = [C.c_void_p]
+    lib.lumen_cloud_get_gaussian.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
+    lib.lumen_cloud_destroy.argtypes = [C.c_void_p]
+
+    def dump(cloud):
+        n = lib.lumen_cloud_get_count(cloud)
+        out = np.zeros((n, 59), np.float32)
+        buf = (C.c_float * 59)()
+        for i in range(n):
+            lib.lumen_cloud_get_gaussian(cloud, i, buf)
+            out[i] = np.frombuffer(buf, dtype=np.float32)
+        lib.lumen_cloud_destroy(cloud)
+        return out
+
+    np.savez_compressed(os.path.join(HERE, "capi_synthetic.npz"),
+                        cube_4_2=dump(lib.lumen_create_synthetic_cube(4, 2.0)),
+                        **{"sphere_128_1.5": dump(lib.lumen_create_synthetic_sphere(128, 1.5))})
+
+
+if __name__ == "__main__":
+    main()
