@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: 1080p frames/s of the forward splatting pipeline on B200.
+
+Workload (configuration 1): 1M Gaussians uniform in a 6x4x6 box 8 units
+ahead, 1920x1080, vertical FOV 50 degrees, degree-3 SH, 16x16 tiles,
+millimetre depth keys, compositing stops at accumulated alpha >= 0.99.
+Synthetic seeded data (numpy PCG64, seed 1); parameters stay resident in HBM.
+
+A step is one full frame: project + cull + SH + scan + key emit, histogram,
+stable digit passes, tile ranges, compositing. ``value`` times K back-to-back
+frames on the device with CUDA events (inputs resident; the 236 MB of
+parameters per frame exceed the 126 MB L2). ``e2e`` times the same frame
+through the reference-facing C ABI call lumen_rasterize with a host frame
+buffer (upload of the buffer's old contents, render, read-back of rgb8,
+depth and alpha inside the timed region; the cloud is uploaded once, in the
+warm-up, as the reference keeps it resident).
+
+``--impl reference`` times the reference's CPU algorithm (the oracle
+restatement of the Mojo path; the Mojo toolchain does not exist here) on all
+host cores for the same workload. Under torchrun N > 1 every rank renders an
+independent replica (the path has no exchange step); value = total frames/s.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p frames/s and p99 latency, served vs per-call render; fwd+bwd steps/s"
+UNIT = "frames/s"
+N_GAUSSIANS = 1_000_000
+WIDTH, HEIGHT = 1920, 1080
+KERNELS_PER_FRAME = 12   # project_emit, histogram, 8 digit passes, tile_ranges, composite
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["lumen", "reference"], default="lumen")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(extra=None):
+    c = {"workload": "config 1: 1M Gaussians, 1920x1080, per-call forward render",
+         "n_gaussians": N_GAUSSIANS, "width": WIDTH, "height": HEIGHT, "sh_degree": 3, "tile": 16,
+         "key": "tile<<32 | clamp(int(z*1000))", "termination": "accumulated alpha >= 0.99",
+         "l2": "inputs larger than L2 (236 MB parameters per frame)", "data": "synthetic, numpy PCG64 seed 1"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    """The reference's CPU algorithm (oracle port of the Mojo path), all host threads."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lumen_b200 import scenes
+    from lumen_b200.types import RenderOptions
+    sc = scenes.box_scene(N_GAUSSIANS, seed=1)
+    s, op = sc.activated()
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    opt = RenderOptions(term_mode=1)
+    nt = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        O.render(sc.means, s, sc.quats, op, sc.sh, cam, opt, stages=False, nthreads=nt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.render(sc.means, s, sc.quats, op, sc.sh, cam, opt, stages=False, nthreads=nt)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = 1.0 / dt
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": workload_config({"parallelism": "host threads"}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
+                             "sample": "one full 1080p frame of config 1 per step (1M Gaussians)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lumen_b200 import scenes
+    from lumen_b200.types import RenderOptions
+    sc = scenes.box_scene(N_GAUSSIANS, seed=1)
+    s, op = sc.activated()
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    nt = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.render(sc.means, s, sc.quats, op, sc.sh, cam, RenderOptions(term_mode=1), stages=False, nthreads=nt)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": nt, "kind": "port",
+            "sample": "one full 1080p frame of config 1 (1M Gaussians), oracle on all host threads"}
+
+
+def e2e_rasterize(sc, scales, opac, steps, warmup):
+    """lumen_rasterize (include/lumen.h) with a host frame buffer."""
+    import numpy as np
+    from lumen_b200 import _lib as L
+    lib = L.load()
+    n = sc.n
+    aos = np.zeros((n, 59), np.float32)
+    aos[:, 0:3] = sc.means
+    aos[:, 3:6] = scales
+    aos[:, 6:10] = sc.quats
+    aos[:, 10] = opac
+    aos[:, 11:59] = sc.sh.reshape(n, 48)
+    cloud = lib.lumen_cloud_create(n)
+    L.check(lib.lumen_cloud_append(cloud, aos.ctypes.data_as(C.POINTER(L.LumenGaussian)), n), "cloud_append")
+    cfg = lib.lumen_default_config()
+    cfg.image_width, cfg.image_height = WIDTH, HEIGHT
+    cfg.near_plane, cfg.far_plane, cfg.early_termination_alpha = 0.01, 1000.0, 0.99
+    r = lib.lumen_rasterizer_create(C.byref(cfg))
+    fb = lib.lumen_framebuffer_create(WIDTH, HEIGHT)
+    cam = L.LumenCamera(L.LumenVec3(0, 0, 0), L.LumenVec3(0, 0, 1), L.LumenVec3(0, -1, 0), 60.0, 50.0, 0.01, 1000.0)
+    st = L.LumenStats()
+    for _ in range(warmup):
+        lib.lumen_framebuffer_clear(fb, 0, 0, 0)
+        L.check(lib.lumen_rasterize(r, cloud, C.byref(cam), fb, C.byref(st)), "rasterize")
+    gpu_ms, wall = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        L.check(lib.lumen_rasterize(r, cloud, C.byref(cam), fb, C.byref(st)), "rasterize")
+        wall.append(time.perf_counter() - t0)
+        gpu_ms.append(st.rasterize_time_ms)
+    npix = WIDTH * HEIGHT
+    out = {"value": 1000.0 / (sum(gpu_ms) / len(gpu_ms)), "unit": UNIT,
+           "h2d_bytes_per_step": npix * 3 + npix * 4, "d2h_bytes_per_step": npix * 3 + npix * 4 + npix * 4,
+           "api": "lumen_rasterize (include/lumen.h), host LumenFrameBuffer",
+           "wall_frames_per_s": 1.0 / (sum(wall) / len(wall)),
+           "p50_ms": statistics.median(gpu_ms), "p99_ms": sorted(gpu_ms)[min(len(gpu_ms) - 1, int(0.99 * len(gpu_ms)))],
+           "visible": int(st.visible_splats), "touched_tiles": int(st.touched_tiles)}
+    lib.lumen_framebuffer_destroy(fb)
+    lib.lumen_rasterizer_destroy(r)
+    lib.lumen_cloud_destroy(cloud)
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    from lumen_b200 import _lib as L
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    from lumen_b200.types import RenderOptions
+
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else open(os.devnull) as f:
+        try:
+            peaks = json.load(f)
+        except ValueError:
+            peaks = {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    sc = scenes.box_scene(N_GAUSSIANS, seed=1)
+    scales, opac = sc.activated()
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    opt = RenderOptions(term_mode=1)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    means, sc_t, quats, op_t, sh = t(sc.means), t(scales), t(sc.quats), t(opac), t(sc.sh).reshape(-1, 48)
+
+    # first render sizes the frame buffers and gives V, K for the byte counts
+    first = R.render(means, sc_t, quats, op_t, sh, cam, opt)
+    frame = first.frame
+    V, K, T = first.n_visible, first.n_instances, cam.n_tiles
+    passes = bin(first.varying_digits).count("1")
+    lib = L.load()
+    g = R.gaussians_struct(means, sc_t, quats, op_t, sh)
+    ccam, copt = L.view_camera(cam), L.render_options(opt)
+    fs = frame.c_struct()
+    img = L.LumenGpuImage()
+    rgb = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, device=dev)
+    depth = torch.empty((HEIGHT, WIDTH), dtype=torch.float32, device=dev)
+    alpha = torch.empty((HEIGHT, WIDTH), dtype=torch.float32, device=dev)
+    img.rgb, img.depth, img.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    timer = lib.lumen_gpu_stage_timer_create(max(args.steps, 1))
+
+    for _ in range(args.warmup):
+        L.check(lib.lumen_gpu_render_forward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs), C.byref(img),
+                                             stream), "forward")
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            L.check(lib.lumen_gpu_render_forward_timed(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs),
+                                                       C.byref(img), timer, stream), "forward")
+        stage = (C.c_float * 4)()
+        total = C.c_float(0)
+        nfr = C.c_int(0)
+        L.check(lib.lumen_gpu_stage_timer_read(timer, stage, C.byref(total), C.byref(nfr)), "timer")
+        torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    counts = L.LumenGpuCounts()
+    L.check(lib.lumen_gpu_read_counts(C.byref(fs), C.byref(counts), stream), "counts")
+    assert counts.error_flags == 0, f"device flags {counts.error_flags:#x}"
+    assert counts.n_instances == K
+    lib.lumen_gpu_stage_timer_destroy(timer)
+    steps = args.steps
+    # first-to-last event span over the K back-to-back frames (gaps included)
+    ms = total.value / steps
+    ms_t = torch.tensor([ms], device=dev)
+    if pg:
+        pg.all_reduce(ms_t, op=pg.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * 1000.0 / ms_max
+
+    stage_ms = [x / steps for x in stage]
+    names = ["project_emit", "sort", "tile_ranges", "composite"]
+    # algorithmic bytes per launch (roofline section)
+    P = WIDTH * HEIGHT
+    alg = {"project_emit": 236 * N_GAUSSIANS + 4 * N_GAUSSIANS + 52 * V + 12 * K,
+           "sort": 8 * K + 24 * K * passes,
+           "tile_ranges": 8 * K + 8 * T,
+           "composite": 40 * K + 16 * P}
+    dom = max(range(4), key=lambda i: stage_ms[i])
+    dname = names[dom]
+    achieved = alg[dname] / (stage_ms[dom] * 1e-3) / 1e9
+    b_fwd = 244 * N_GAUSSIANS + 64 * V + (68 + 24 * passes) * K + 8 * T + 16 * P
+    frame_gbs = b_fwd / (ms_max * 1e-3) / 1e9
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": workload_config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+            "gpu_launches": KERNELS_PER_FRAME * steps,
+            "clocks": clk.summary(),
+            "stages_ms": {n: round(v, 4) for n, v in zip(names, stage_ms)},
+            "counts": {"visible": V, "instances": K, "tiles": T, "digit_passes": passes},
+            "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                         "algorithmic_bytes": alg[dname]},
+            "frame_roofline": {"bytes": b_fwd, "achieved": frame_gbs, "peak": hbm_peak, "unit": "GB/s",
+                               "frac": frame_gbs / hbm_peak}}
+    if not args.no_e2e:
+        e2e = e2e_rasterize(sc, scales, opac, steps, args.warmup)
+        if pg:   # replicas: the slowest rank's rate times the number of ranks
+            v = torch.tensor([e2e["value"]], device=dev)
+            pg.all_reduce(v, op=pg.ReduceOp.MIN)
+            e2e["value"] = float(v.item()) * world
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -126,6 +126,7 @@ typedef struct {
 #define LUMEN_GPU_ERR_CAPACITY 1u
 #define LUMEN_GPU_ERR_SPIN_TIMEOUT 2u
 #define LUMEN_GPU_ERR_LAUNCH 4u
+#define LUMEN_GPU_ERR_BOUNDS 8u   /* a device-side index check failed; the access was skipped */
 
 /* Bytes of scratch a frame needs (control block, look-back descriptors,
  * digit histograms). */
@@ -160,6 +161,23 @@ const LumenGpuFrame* lumen_gpu_renderer_frame(const LumenGpuRenderer* renderer);
 LumenStatus lumen_gpu_sort_pairs(uint64_t* keys0, uint32_t* vals0, uint64_t* keys1, uint32_t* vals1,
                                  int64_t n, void* scratch, size_t scratch_bytes, uint32_t* sorted_buffer,
                                  void* stream);
+
+/* Stage timing with CUDA events on the render stream. A timer holds events
+ * for up to max_frames frames; each lumen_gpu_render_forward_timed call
+ * records 5 events (before K1, after K1, after the sort, after the ranges,
+ * after compositing) into the next frame slot without waiting.
+ * lumen_gpu_stage_timer_read waits for the last event and returns the summed
+ * milliseconds of the 4 stages over the recorded frames, then resets.
+ * No counterpart in the reference (its timers are perf_counter_ns and clock(),
+ * src/main.mojo:105-108, c_api/src/lumen_c.c:389,561). */
+typedef struct LumenGpuStageTimer LumenGpuStageTimer;
+LumenGpuStageTimer* lumen_gpu_stage_timer_create(int max_frames);
+void lumen_gpu_stage_timer_destroy(LumenGpuStageTimer* timer);
+LumenStatus lumen_gpu_render_forward_timed(const LumenGpuGaussians* gaussians, const LumenViewCamera* camera,
+                                           const LumenRenderOptions* options, LumenGpuFrame* frame,
+                                           LumenGpuImage* image, LumenGpuStageTimer* timer, void* stream);
+LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms[4], float* total_ms,
+                                       int* n_frames);
 
 /* Append n splats to a cloud in one copy. No counterpart in the reference:
  * the bulk form of lumen_cloud_add_gaussian (c_api/include/lumen.h:129),

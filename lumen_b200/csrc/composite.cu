@@ -29,7 +29,7 @@ struct CompositeSmem {
 
 __global__ void __launch_bounds__(kTilePixels)
 composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, long long capacity,
-                 const Control* __restrict__ ctrl, int width, int height, int tiles_x,
+                 Control* __restrict__ ctrl, int width, int height, int tiles_x,
                  LumenRenderOptions opt, LumenGpuImage img) {
     __shared__ CompositeSmem s;
     const int tile = blockIdx.x;
@@ -49,7 +49,13 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
         /* pipeline.mojo:162-163: no instances, the output stays zero */
         background = false;
     } else {
-        const int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
+        int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
+        const unsigned int n_visible = ctrl->n_visible;
+        if (!(rs == -1 || rs >= re) && (rs < 0 || (long long)re > K)) {
+            /* self-check: a range outside the sorted instances */
+            if (tid == 0) atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+            rs = re = -1;
+        }
         if (!(rs == -1 || rs >= re)) {
             const unsigned int* __restrict__ vals = ctrl->sorted_buffer ? f.vals[1] : f.vals[0];
             const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
@@ -60,10 +66,18 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
                 if (__syncthreads_count(!done) == 0) break;
                 const int i = cs + tid;
                 if (i < re) {
-                    const float4* r4 = reinterpret_cast<const float4*>(records + vals[i]);
-                    s.geo[tid] = __ldg(r4);
-                    s.con[tid] = __ldg(r4 + 1);
-                    s.col[tid] = __ldg(r4 + 2);
+                    unsigned int v = vals[i];
+                    if (v >= n_visible) {   /* self-check: an index beyond the visible records */
+                        atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+                        s.geo[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        s.con[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        s.col[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    } else {
+                        const float4* r4 = reinterpret_cast<const float4*>(records + v);
+                        s.geo[tid] = __ldg(r4);
+                        s.con[tid] = __ldg(r4 + 1);
+                        s.col[tid] = __ldg(r4 + 2);
+                    }
                 }
                 __syncthreads();
                 const int n = re - cs < kTilePixels ? re - cs : kTilePixels;
@@ -115,7 +129,7 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
     if (img.last_idx) img.last_idx[pix] = last;
 }
 
-void launch_composite(const LumenGpuFrame& f, const Control* ctrl, const LumenViewCamera& cam,
+void launch_composite(const LumenGpuFrame& f, Control* ctrl, const LumenViewCamera& cam,
                       const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st) {
     const int tiles_x = (cam.width + kTile - 1) / kTile;
     const int tiles_y = (cam.height + kTile - 1) / kTile;

@@ -24,9 +24,9 @@ void launch_project_emit(const LumenGpuGaussians& g, const LumenViewCamera& cam,
                          LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, cudaStream_t st);
 void launch_sort(LumenGpuFrame& f, Control* ctrl, unsigned int* sort_lb, long long lb_tiles_cap,
                  long long n_range_ints, int num_sms, cudaStream_t st);
-void launch_ranges(LumenGpuFrame& f, Control* ctrl, int num_sms, cudaStream_t st);
+void launch_ranges(LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st);
 void launch_key_stats(const unsigned long long* keys, long long n, Control* ctrl, int num_sms, cudaStream_t st);
-void launch_composite(const LumenGpuFrame& f, const Control* ctrl, const LumenViewCamera& cam,
+void launch_composite(const LumenGpuFrame& f, Control* ctrl, const LumenViewCamera& cam,
                       const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st);
 void configure_sort_kernels();
 
@@ -96,9 +96,86 @@ size_t lumen_gpu_scratch_bytes(int64_t n_gaussians, int64_t instance_capacity, i
     return ScratchLayout::make(n_gaussians, instance_capacity).total;
 }
 
+}  // extern "C"
+
+struct LumenGpuStageTimer {
+    int max_frames = 0;
+    int next = 0;
+    cudaEvent_t* ev = nullptr;   /* max_frames x 5 */
+};
+
+namespace lumen {
+
+static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
+                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream);
+
+}  // namespace lumen
+
+extern "C" {
+
 LumenStatus lumen_gpu_render_forward(const LumenGpuGaussians* g, const LumenViewCamera* cam,
                                      const LumenRenderOptions* opt, LumenGpuFrame* f, LumenGpuImage* img,
                                      void* stream) {
+    return forward_impl(g, cam, opt, f, img, nullptr, stream);
+}
+
+LumenGpuStageTimer* lumen_gpu_stage_timer_create(int max_frames) {
+    if (max_frames <= 0) return nullptr;
+    LumenGpuStageTimer* t = new (std::nothrow) LumenGpuStageTimer();
+    if (!t) return nullptr;
+    t->ev = new (std::nothrow) cudaEvent_t[(size_t)max_frames * 5]();
+    if (!t->ev) { delete t; return nullptr; }
+    t->max_frames = max_frames;
+    for (int i = 0; i < max_frames * 5; ++i)
+        if (cudaEventCreate(&t->ev[i]) != cudaSuccess) { lumen_gpu_stage_timer_destroy(t); return nullptr; }
+    return t;
+}
+
+void lumen_gpu_stage_timer_destroy(LumenGpuStageTimer* t) {
+    if (!t) return;
+    if (t->ev)
+        for (int i = 0; i < t->max_frames * 5; ++i)
+            if (t->ev[i]) cudaEventDestroy(t->ev[i]);
+    delete[] t->ev;
+    delete t;
+}
+
+LumenStatus lumen_gpu_render_forward_timed(const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                           const LumenRenderOptions* opt, LumenGpuFrame* f, LumenGpuImage* img,
+                                           LumenGpuStageTimer* t, void* stream) {
+    if (!t || t->next >= t->max_frames) return LUMEN_ERROR_INVALID_ARGUMENT;
+    LumenStatus st = forward_impl(g, cam, opt, f, img, t->ev + (size_t)t->next * 5, stream);
+    if (st == LUMEN_SUCCESS) t->next++;
+    return st;
+}
+
+LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* t, float stage_ms[4], float* total_ms, int* n_frames) {
+    if (!t || !stage_ms) return LUMEN_ERROR_INVALID_ARGUMENT;
+    for (int s = 0; s < 4; ++s) stage_ms[s] = 0.0f;
+    if (total_ms) *total_ms = 0.0f;
+    if (n_frames) *n_frames = t->next;
+    if (t->next == 0) return LUMEN_SUCCESS;
+    cudaError_t e = cudaEventSynchronize(t->ev[(size_t)(t->next - 1) * 5 + 4]);
+    if (e != cudaSuccess) return map_cuda(e);
+    for (int fr = 0; fr < t->next; ++fr) {
+        cudaEvent_t* ev = t->ev + (size_t)fr * 5;
+        for (int s = 0; s < 4; ++s) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[s], ev[s + 1]);
+            stage_ms[s] += ms;
+        }
+    }
+    if (total_ms) cudaEventElapsedTime(total_ms, t->ev[0], t->ev[(size_t)(t->next - 1) * 5 + 4]);
+    t->next = 0;
+    return LUMEN_SUCCESS;
+}
+
+}  // extern "C"
+
+namespace lumen {
+
+static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
+                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream) {
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
     if (!f || !img || !img->rgb || !f->scratch || !f->ranges || f->instance_capacity <= 0 ||
@@ -113,17 +190,26 @@ LumenStatus lumen_gpu_render_forward(const LumenGpuGaussians* g, const LumenView
     Control* ctrl = (Control*)(base + L.control_off);
     unsigned long long* plb = (unsigned long long*)(base + L.proj_lb_off);
     unsigned int* slb = (unsigned int*)(base + L.sort_lb_off);
+    if (ev) cudaEventRecord(ev[0], s);
     cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
     if (e != cudaSuccess) return map_cuda(e);
     if (g->count > 0) launch_project_emit(*g, *cam, *opt, *f, ctrl, plb, (int)L.proj_blocks, s);
+    if (ev) cudaEventRecord(ev[1], s);
     const long long tiles = (long long)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
     const int sms = device_sm_count();
     launch_sort(*f, ctrl, slb, L.sort_tiles, 2 * tiles, sms, s);
-    launch_ranges(*f, ctrl, sms, s);
+    if (ev) cudaEventRecord(ev[2], s);
+    launch_ranges(*f, ctrl, tiles, sms, s);
+    if (ev) cudaEventRecord(ev[3], s);
     launch_composite(*f, ctrl, *cam, *opt, *img, s);
+    if (ev) cudaEventRecord(ev[4], s);
     e = cudaGetLastError();
     return map_cuda(e);
 }
+
+}  // namespace lumen
+
+extern "C" {
 
 LumenStatus lumen_gpu_read_counts(const LumenGpuFrame* f, LumenGpuCounts* c, void* stream) {
     if (!f || !c || !f->scratch) return LUMEN_ERROR_INVALID_ARGUMENT;

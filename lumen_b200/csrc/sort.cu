@@ -255,13 +255,17 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
  * appears in the sorted keys and ends after it last appears. Ranges were
  * filled with -1 by the histogram kernel (empty tiles stay (-1, -1)). */
 __global__ void __launch_bounds__(256)
-tile_ranges_kernel(LumenGpuFrame f, long long capacity, Control* ctrl) {
+tile_ranges_kernel(LumenGpuFrame f, long long capacity, long long n_tiles, Control* ctrl) {
     const long long K = effective_count(ctrl, capacity);
     const unsigned long long* __restrict__ keys = reinterpret_cast<const unsigned long long*>(ctrl->sorted_buffer ? f.keys[1] : f.keys[0]);
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     unsigned int touched = 0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < K; i += nthreads) {
         const unsigned int t = (unsigned int)(keys[i] >> 32);
+        if ((long long)t >= n_tiles) {   /* self-check: a tile id outside the grid */
+            atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+            continue;
+        }
         const bool first = i == 0 || (unsigned int)(keys[i - 1] >> 32) != t;
         const bool last = i == K - 1 || (unsigned int)(keys[i + 1] >> 32) != t;
         if (first) { f.ranges[2 * (size_t)t] = (int)i; ++touched; }
@@ -284,8 +288,8 @@ void launch_sort(LumenGpuFrame& f, Control* ctrl, unsigned int* sort_lb, long lo
         onesweep_pass_kernel<<<num_sms * 2, kSortThreads, smem, st>>>(f, cap, ctrl, sort_lb, lb_tiles_cap, d);
 }
 
-void launch_ranges(LumenGpuFrame& f, Control* ctrl, int num_sms, cudaStream_t st) {
-    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f, (long long)f.instance_capacity, ctrl);
+void launch_ranges(LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st) {
+    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f, (long long)f.instance_capacity, n_tiles, ctrl);
 }
 
 /* OR and OR-of-complement of n keys, for a sort whose keys were not emitted
