@@ -39,14 +39,14 @@ METRIC = "1080p frames/s and p99 latency, served vs per-call render; fwd+bwd ste
 UNIT = "frames/s"
 N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
-KERNELS_PER_FRAME = 12   # project_emit, histogram, 8 digit passes, tile_ranges, composite
+KERNELS_PER_FRAME = 13   # project, 2 x (histogram + 4 digit passes), emit, tile_ranges, composite
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=30)
-    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["lumen", "reference"], default="lumen")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -64,56 +64,58 @@ def workload_config(extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
-    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
-             "clocks_event_reasons.sw_power_cap"
+    """SM clock and clock-event reasons sampled through NVML every 10 ms while
+    the timed region runs (nvidia-smi's -lms loop as a fallback)."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = cuda_index
+        if vis:
+            try:
+                idx = int(vis.split(",")[cuda_index])
+            except (ValueError, IndexError):
+                pass
+        self.index = idx
+        self.sm, self.reasons, self.max = [], 0, None
+        self.stop = threading.Event()
+        self.nvml = None
+
+    def _loop(self):
+        h = self.nvml.nvmlDeviceGetHandleByIndex(self.index)
+        self.max = self.nvml.nvmlDeviceGetMaxClockInfo(h, self.nvml.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                self.sm.append(self.nvml.nvmlDeviceGetClockInfo(h, self.nvml.NVML_CLOCK_SM))
+                self.reasons |= int(self.nvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.t = threading.Thread(target=self._loop, daemon=True)
             self.t.start()
-        except OSError:
-            self.proc = None
+            deadline = time.time() + 2.0
+            while not self.sm and time.time() < deadline:
+                time.sleep(0.005)
+        except Exception:
+            self.nvml = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.nvml:
+            self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 8:
-                continue
-            try:
-                sm.append(float(f[0]))
-                mx = float(f[1])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[4:8]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.max,
+                "reasons": sorted(v for k, v in self.REASONS.items() if self.reasons & k),
+                "samples": len(self.sm), "source": "nvml, 10 ms"}
 
 
 def dist_setup():
@@ -254,7 +256,9 @@ def main():
     first = R.render(means, sc_t, quats, op_t, sh, cam, opt)
     frame = first.frame
     V, K, T = first.n_visible, first.n_instances, cam.n_tiles
-    passes = bin(first.varying_digits).count("1")
+    # bytes of the reference's 64-bit key that vary: tile-id bytes (low 8 bits of the mask,
+    # key bytes 4..7) and depth-key bytes (next 8 bits, key bytes 0..3)
+    passes = bin(first.varying_digits & 0xFFFF).count("1")
     lib = L.load()
     g = R.gaussians_struct(means, sc_t, quats, op_t, sh)
     ccam, copt = L.view_camera(cam), L.render_options(opt)
@@ -300,11 +304,13 @@ def main():
     value = world * 1000.0 / ms_max
 
     stage_ms = [x / steps for x in stage]
-    names = ["project_emit", "sort", "tile_ranges", "composite"]
-    # algorithmic bytes per launch (roofline section)
+    names = ["project", "sort", "tile_ranges", "composite"]
+    # algorithmic bytes per launch (roofline section); p = digit passes of the
+    # reference's 64-bit key sort that vary (its 8-pass sort with constant digits skipped)
     P = WIDTH * HEIGHT
-    alg = {"project_emit": 236 * N_GAUSSIANS + 4 * N_GAUSSIANS + 52 * V + 12 * K,
-           "sort": 8 * K + 24 * K * passes,
+    p = passes
+    alg = {"project": 236 * N_GAUSSIANS + 48 * V + 4 * N_GAUSSIANS,
+           "sort": 8 * N_GAUSSIANS + 16 * V + 12 * K + 8 * K + 24 * K * p,
            "tile_ranges": 8 * K + 8 * T,
            "composite": 40 * K + 16 * P}
     dom = max(range(4), key=lambda i: stage_ms[i])

@@ -80,15 +80,29 @@ typedef struct {
 } LumenSplatRecord;
 
 /* Work buffers of one frame, device memory owned by the caller.
- * records/visible_ids/radii hold n_gaussians entries; keys/vals hold
- * instance_capacity entries each (two ping-pong sets); ranges holds
- * 2 * n_tiles int32 (start, end; -1,-1 for an empty tile, as
- * binning.mojo:10-28); scratch is lumen_gpu_scratch_bytes() bytes. */
+ *
+ * The reference sorts 64-bit (tile << 32 | depth key) instance keys with a
+ * stable LSD sort over emission order (pipeline.mojo:152-166). The same
+ * permutation is produced here in two smaller sorts: the visible splats are
+ * stably sorted by depth key (depth_keys/depth_order), instances are emitted
+ * in that order with 32-bit tile-id keys, and those are stably sorted by
+ * tile (keys/vals). Within a tile both orders are (depth key, visible index).
+ *
+ * Per Gaussian (n_gaussians entries each): records, visible_ids, radii,
+ * rects (tile rectangle of each visible splat: min_tx | min_ty << 16 |
+ * max_tx << 32 | max_ty << 48), depth_keys[2] and depth_order[2] (ping-pong).
+ * Per instance (instance_capacity entries each): keys[2] (tile ids) and
+ * vals[2] (visible indices), ping-pong. ranges: 2 * n_tiles int32 (start,
+ * end; -1,-1 for an empty tile, as binning.mojo:10-28). scratch:
+ * lumen_gpu_scratch_bytes() bytes. */
 typedef struct {
     LumenSplatRecord* records;
     uint32_t* visible_ids;
     int32_t* radii;
-    uint64_t* keys[2];
+    uint64_t* rects;
+    uint32_t* depth_keys[2];
+    uint32_t* depth_order[2];
+    uint32_t* keys[2];
     uint32_t* vals[2];
     int64_t instance_capacity;
     int32_t* ranges;
@@ -111,9 +125,11 @@ typedef struct {
 /* Frame counters read back by lumen_gpu_read_counts. error_flags bits:
  * 1 = instances exceeded instance_capacity (outputs invalid; re-run with a
  *     larger frame), 2 = a bounded spin-wait gave up (outputs invalid),
- * 4 = invalid launch parameters. sorted_buffer: which of keys[0]/keys[1]
- * holds the sorted keys. varying_digits: bit d set when byte d of the keys
- * varies (only those digit passes run). */
+ * 4 = invalid launch parameters, 8 = a device-side index check failed.
+ * sorted_buffer: which of keys/vals [0] or [1] holds the tile-sorted
+ * instances; depth_sorted_buffer: the same for depth_keys/depth_order.
+ * varying_digits: bit d set when byte d of the tile ids varies, bit 8+d when
+ * byte d of the depth keys varies (only those digit passes run). */
 typedef struct {
     int64_t n_visible;
     int64_t n_instances;
@@ -121,6 +137,8 @@ typedef struct {
     uint32_t sorted_buffer;
     uint32_t varying_digits;
     uint32_t touched_tiles;
+    uint32_t depth_sorted_buffer;
+    uint32_t reserved;
 } LumenGpuCounts;
 
 #define LUMEN_GPU_ERR_CAPACITY 1u
@@ -153,6 +171,13 @@ LumenStatus lumen_gpu_renderer_render(LumenGpuRenderer* renderer, const LumenGpu
                                       LumenGpuImage* image, LumenGpuCounts* counts, void* stream);
 /* The renderer's frame (valid after a render; for inspection and backward). */
 const LumenGpuFrame* lumen_gpu_renderer_frame(const LumenGpuRenderer* renderer);
+
+/* The reference's sorted 64-bit keys (tile << 32 | depth key), rebuilt from
+ * a finished frame's tile-sorted instances: out[i] for i < n_instances.
+ * For inspection and parity checks; the pipeline itself never forms them.
+ * Waits. */
+LumenStatus lumen_gpu_frame_sorted_keys64(const LumenGpuFrame* frame, const LumenRenderOptions* options,
+                                          uint64_t* out, void* stream);
 
 /* Stable sort of n (key, value) pairs by key, in place in keys[0]/vals[0]
  * with keys[1]/vals[1] as the alternate buffers; the sorted data ends in the

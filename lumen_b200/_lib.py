@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "SUCCESS", -1: "INVALID_ARGUMENT", -2: "OUT_OF_MEMORY", -3: "
 ERR_CAPACITY = 1
 ERR_SPIN_TIMEOUT = 2
 ERR_LAUNCH = 4
+ERR_BOUNDS = 8
 
 
 class LumenError(RuntimeError):
@@ -88,8 +89,9 @@ class LumenRenderOptions(C.Structure):
 
 
 class LumenGpuFrame(C.Structure):
-    _fields_ = [("records", _P), ("visible_ids", _P), ("radii", _P), ("keys", _P * 2), ("vals", _P * 2),
-                ("instance_capacity", C.c_int64), ("ranges", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t)]
+    _fields_ = [("records", _P), ("visible_ids", _P), ("radii", _P), ("rects", _P), ("depth_keys", _P * 2),
+                ("depth_order", _P * 2), ("keys", _P * 2), ("vals", _P * 2), ("instance_capacity", C.c_int64),
+                ("ranges", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t)]
 
 
 class LumenGpuImage(C.Structure):
@@ -98,7 +100,8 @@ class LumenGpuImage(C.Structure):
 
 class LumenGpuCounts(C.Structure):
     _fields_ = [("n_visible", C.c_int64), ("n_instances", C.c_int64), ("error_flags", C.c_uint32),
-                ("sorted_buffer", C.c_uint32), ("varying_digits", C.c_uint32), ("touched_tiles", C.c_uint32)]
+                ("sorted_buffer", C.c_uint32), ("varying_digits", C.c_uint32), ("touched_tiles", C.c_uint32),
+                ("depth_sorted_buffer", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 SPLAT_RECORD_BYTES = 48
@@ -141,6 +144,7 @@ SIGNATURES = {
                                             C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuImage),
                                             C.POINTER(LumenGpuCounts), _P]),
     "lumen_gpu_renderer_frame": (C.POINTER(LumenGpuFrame), [_P]),
+    "lumen_gpu_frame_sorted_keys64": (C.c_int, [C.POINTER(LumenGpuFrame), C.POINTER(LumenRenderOptions), _P, _P]),
     "lumen_gpu_sort_pairs": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, C.c_size_t, C.POINTER(C.c_uint32), _P]),
     "lumen_cloud_append": (C.c_int, [_P, C.POINTER(LumenGaussian), C.c_size_t]),
     "lumen_gpu_stage_timer_create": (_P, [C.c_int]),

@@ -5,13 +5,15 @@
  * src/raster/pipeline.mojo:172-229, with compute_gaussian_pixel_alpha and
  * PixelAccumulator.blend/finalize, src/raster/compositor.mojo:10-89.
  *
- * One CTA per 16x16 tile, one thread per pixel. The tile's sorted instances
- * are processed in chunks of 256: each thread gathers one instance's
- * 48-byte record (through the sorted visible index) into shared memory,
- * then every thread walks the chunk in order, so each pixel blends its
- * splats in exactly the reference order. A pixel stops after the blend that
- * saturates it; a warp leaves the chunk once all its pixels stopped, and the
- * CTA stops loading chunks once all 256 pixels stopped.
+ * One CTA per 16x16 tile, one thread per pixel, each warp an 8x4 block. The
+ * tile's sorted instances are processed in chunks of 256: each thread
+ * gathers one instance's 48-byte record (through the sorted visible index)
+ * into shared memory and computes which warp blocks the splat can reach at
+ * all (reach_mask); each warp then walks, in sorted order, only the splats
+ * that can reach it, so each pixel blends exactly the reference's sequence.
+ * A pixel stops after the blend that saturates it; a warp leaves the chunk
+ * once all its pixels stopped, and the CTA stops loading chunks once all 256
+ * pixels stopped.
  *
  * Built with --fmad=false: power, alpha, weights and transmittance round as
  * in the reference, so contributor counts match the CPU restatement bit for
@@ -22,20 +24,69 @@
 namespace lumen {
 
 struct CompositeSmem {
-    float4 geo[kTilePixels];   /* cx, cy, depth, opacity */
-    float4 con[kTilePixels];   /* ic00, ic01, ic11, - */
-    float4 col[kTilePixels];   /* r, g, b, - */
+    float4 geo[kTilePixels];            /* cx, cy, depth, opacity */
+    float4 con[kTilePixels];            /* ic00, ic01, ic11, - */
+    float4 col[kTilePixels];            /* r, g, b, - */
+    unsigned char mask[kTilePixels];    /* bit w: the splat can reach warp w's pixels */
+    unsigned short list[kTilePixels / 32][kTilePixels];
 };
 
-__global__ void __launch_bounds__(kTilePixels)
+/* Warp w of a tile shades an 8x4 block of pixels. */
+__device__ __forceinline__ int warp_block_x(int w) { return (w & 1) * 8; }
+__device__ __forceinline__ int warp_block_y(int w) { return (w >> 1) * 4; }
+
+/* Minimum of q(x, y) = a x^2 + 2 b x y + c y^2 over [x0,x1] x [y0,y1]
+ * (a > 0, c > 0, ac > b^2): 0 if the origin is inside, otherwise the least
+ * of the four edge minima (q is convex along each edge). */
+__device__ __forceinline__ float quad_min_rect(float a, float b, float c, float x0, float x1, float y0, float y1) {
+    if (x0 <= 0.0f && x1 >= 0.0f && y0 <= 0.0f && y1 >= 0.0f) return 0.0f;
+    float m = INFINITY;
+    const float xs[2] = {x0, x1}, ys[2] = {y0, y1};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float x = xs[k];
+        const float y = fminf(fmaxf(-b * x / c, y0), y1);
+        m = fminf(m, a * x * x + 2.0f * b * x * y + c * y * y);
+        const float yy = ys[k];
+        const float xx = fminf(fmaxf(-b * yy / a, x0), x1);
+        m = fminf(m, a * xx * xx + 2.0f * b * xx * yy + c * yy * yy);
+    }
+    return m;
+}
+
+/* Bit w set when the splat may reach the blend threshold at some pixel
+ * centre of warp w's block. A pixel is blended only if
+ * power <= 4.5 and opacity * exp(-power) >= 1/255 (compositor.mojo:62-89,
+ * :33-35), i.e. 2 * power <= 2 * min(4.5, ln(255 * opacity)); the test uses
+ * that bound with a 0.1% + 0.01 margin, far above the float rounding of
+ * power, so culling never removes a splat that the per-pixel loop would
+ * blend and the results are unchanged. */
+__device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float tile_x0, float tile_y0) {
+    const float a = con.x, b = con.y, c = con.z, op = geo.w;
+    if (!(a > 0.0f && c > 0.0f && a * c - b * b > 0.0f) || !isfinite(a * c)) return 0xFFu;
+    const float pcut = fminf(4.5f, __logf(op / min_alpha()) + 0.01f);
+    if (pcut < 0.0f) return 0u;
+    const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
+    unsigned int m = 0;
+#pragma unroll
+    for (int w = 0; w < kTilePixels / 32; ++w) {
+        const float x0 = tile_x0 + (float)warp_block_x(w) + 0.5f - geo.x;
+        const float y0 = tile_y0 + (float)warp_block_y(w) + 0.5f - geo.y;
+        if (quad_min_rect(a, b, c, x0, x0 + 7.0f, y0, y0 + 3.0f) <= qcut) m |= 1u << w;
+    }
+    return m;
+}
+
+__global__ void __launch_bounds__(kTilePixels, 6)
 composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, long long capacity,
                  Control* __restrict__ ctrl, int width, int height, int tiles_x,
                  LumenRenderOptions opt, LumenGpuImage img) {
     __shared__ CompositeSmem s;
     const int tile = blockIdx.x;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
-    const int px = tx * kTile + (tid & 15), py = ty * kTile + (tid >> 4);
+    const int px = tx * kTile + warp_block_x(warp) + (lane & 7);
+    const int py = ty * kTile + warp_block_y(warp) + (lane >> 3);
     const bool inside = px < width && py < height;
     const long long pix = (long long)py * width + px;
     const long long K = (long long)ctrl->n_instances < capacity ? (long long)ctrl->n_instances : capacity;
@@ -57,33 +108,45 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
             rs = re = -1;
         }
         if (!(rs == -1 || rs >= re)) {
-            const unsigned int* __restrict__ vals = ctrl->sorted_buffer ? f.vals[1] : f.vals[0];
+            const unsigned int* __restrict__ vals = ctrl->tile_sort.sorted_buffer ? f.vals[1] : f.vals[0];
             const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+            const float tile_x0 = (float)(tx * kTile), tile_y0 = (float)(ty * kTile);
             const float thr = opt.term_threshold;
             const bool mode_alpha = opt.term_mode == 1;
             bool done = !inside;
             for (int cs = rs; cs < re; cs += kTilePixels) {
                 if (__syncthreads_count(!done) == 0) break;
                 const int i = cs + tid;
+                unsigned int m = 0;
                 if (i < re) {
                     unsigned int v = vals[i];
                     if (v >= n_visible) {   /* self-check: an index beyond the visible records */
                         atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
-                        s.geo[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        s.con[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        s.col[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     } else {
                         const float4* r4 = reinterpret_cast<const float4*>(records + v);
-                        s.geo[tid] = __ldg(r4);
-                        s.con[tid] = __ldg(r4 + 1);
+                        const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
+                        s.geo[tid] = geo;
+                        s.con[tid] = con;
                         s.col[tid] = __ldg(r4 + 2);
+                        m = reach_mask(geo, con, tile_x0, tile_y0);
                     }
                 }
+                s.mask[tid] = (unsigned char)m;
                 __syncthreads();
+                /* this warp's splats of the chunk, in sorted order */
                 const int n = re - cs < kTilePixels ? re - cs : kTilePixels;
-                for (int j = 0; j < n; ++j) {
+                int cnt = 0;
+                for (int base = 0; base < n; base += 32) {
+                    const int j = base + lane;
+                    const bool bit = j < n && ((s.mask[j] >> warp) & 1u);
+                    const unsigned int bal = __ballot_sync(0xffffffffu, bit);
+                    if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned short)j;
+                    cnt += __popc(bal);
+                }
+                __syncwarp();
+                for (int t = 0; t < cnt; ++t) {
+                    const int j = s.list[warp][t];
                     if (!done) {
-                        last = cs + j;
                         const float4 gg = s.geo[j];
                         const float4 cc = s.con[j];
                         /* compute_gaussian_pixel_alpha, compositor.mojo:62-89 */
@@ -107,7 +170,10 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
                                 T *= (1.0f - alpha);
                                 acc = 1.0f - T;
                                 ++count;
-                                if (mode_alpha ? (acc >= thr) : (T <= thr)) done = true;
+                                if (mode_alpha ? (acc >= thr) : (T <= thr)) {
+                                    done = true;
+                                    last = cs + j;
+                                }
                             }
                         }
                     }
@@ -115,6 +181,8 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
                 }
                 __syncthreads();
             }
+            /* a pixel that never saturated visited the whole range */
+            if (!done) last = re - 1;
         }
     }
     if (!inside) return;

@@ -1,15 +1,19 @@
 /*
  * forward.cu - host side of the device API declared in include/lumen_gpu.h:
- * argument checks, scratch layout, the launch sequence of one frame, and a
- * renderer that owns and grows its frame buffers.
+ * argument checks, scratch layout, the launch sequence of one frame, stage
+ * timing, and a renderer that owns and grows its frame buffers.
  *
  * Launch sequence of a frame (all on the caller's stream, no host sync):
- *   memset(control + project look-back)
- *   project_emit      K1 (projection, compacting scan, key emission)
- *   sort_histogram    digit histograms; clears look-back; ranges = -1
- *   onesweep_pass x8  K3 (a pass whose digit is constant exits at once)
- *   tile_ranges       K4
- *   composite         K5
+ *   memset(control + both look-back scans)
+ *   project            K1: projection, cull, SH, compacting scan, depth keys
+ *   histogram<u32>     depth-key digits of the visible splats
+ *   onesweep_pass x4   stable sort of visible splats by depth key
+ *   emit               K2: (tile id, visible index) per covered tile, in depth order
+ *   histogram<u32>     tile-id digits; ranges = -1
+ *   onesweep_pass x4   stable sort of instances by tile id
+ *   tile_ranges        K4
+ *   composite          K5
+ * Passes whose digit is constant exit at once (decided on the device).
  */
 #include <cstdio>
 #include <cstdlib>
@@ -20,12 +24,20 @@
 #include "splat_common.cuh"
 
 namespace lumen {
-void launch_project_emit(const LumenGpuGaussians& g, const LumenViewCamera& cam, const LumenRenderOptions& opt,
-                         LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, cudaStream_t st);
-void launch_sort(LumenGpuFrame& f, Control* ctrl, unsigned int* sort_lb, long long lb_tiles_cap,
-                 long long n_range_ints, int num_sms, cudaStream_t st);
-void launch_ranges(LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st);
-void launch_key_stats(const unsigned long long* keys, long long n, Control* ctrl, int num_sms, cudaStream_t st);
+void launch_project(const LumenGpuGaussians& g, const LumenViewCamera& cam, const LumenRenderOptions& opt,
+                    const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, cudaStream_t st);
+void launch_emit(const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, int tiles_x,
+                 cudaStream_t st);
+void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
+                   SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges, long long n_range_ints,
+                   unsigned int* err, int num_sms, cudaStream_t st);
+void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
+                   long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
+                   int num_sms, cudaStream_t st);
+void launch_ranges(const LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st);
+void launch_key_stats64(const unsigned long long* keys, long long n, SortControl* sc, int num_sms, cudaStream_t st);
+void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_mode, unsigned long long* out,
+                          int num_sms, cudaStream_t st);
 void launch_composite(const LumenGpuFrame& f, Control* ctrl, const LumenViewCamera& cam,
                       const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st);
 void configure_sort_kernels();
@@ -53,6 +65,8 @@ LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam,
     }
     if (cam->width <= 0 || cam->height <= 0 || cam->width > 65535 * kTile || cam->height > 65535 * kTile)
         return LUMEN_ERROR_INVALID_ARGUMENT;
+    const long long tiles = (long long)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
+    if (tiles >= (1ll << 31)) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (opt->tile_size != kTile) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (opt->sh_degree < 0 || opt->sh_degree > 3) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (opt->key_mode < 0 || opt->key_mode > 1 || opt->term_mode < 0 || opt->term_mode > 1)
@@ -61,23 +75,15 @@ LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam,
 }
 
 /* Device-side failures: capacity still exceeded -> out of memory; a bounded
- * wait that gave up or a bad launch -> I/O failure (the device did not
- * complete the frame). */
-static LumenStatus status_from_flags(unsigned int flags) {
+ * wait that gave up, a failed index check or a bad launch -> I/O failure
+ * (the device did not complete the frame correctly). */
+LumenStatus status_from_flags(unsigned int flags) {
     if (flags & LUMEN_GPU_ERR_CAPACITY) return LUMEN_ERROR_OUT_OF_MEMORY;
     if (flags) return LUMEN_ERROR_IO_FAILURE;
     return LUMEN_SUCCESS;
 }
 
-static LumenGpuFrame f_scratch_only(void* scratch, size_t bytes) {
-    LumenGpuFrame f;
-    std::memset(&f, 0, sizeof(f));
-    f.scratch = scratch;
-    f.scratch_bytes = bytes;
-    return f;
-}
-
-static LumenStatus map_cuda(cudaError_t e) {
+LumenStatus map_cuda(cudaError_t e) {
     if (e == cudaSuccess) return LUMEN_SUCCESS;
     if (e == cudaErrorMemoryAllocation) return LUMEN_ERROR_OUT_OF_MEMORY;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInitializationError)
@@ -85,9 +91,65 @@ static LumenStatus map_cuda(cudaError_t e) {
     return LUMEN_ERROR_INVALID_ARGUMENT;
 }
 
+static bool frame_ok(const LumenGpuFrame* f, int64_t n) {
+    if (!f || !f->scratch || !f->ranges || f->instance_capacity <= 0 || f->instance_capacity >= (1ll << 30)) return false;
+    if (!f->keys[0] || !f->keys[1] || !f->vals[0] || !f->vals[1]) return false;
+    if (n > 0 && (!f->records || !f->visible_ids || !f->radii || !f->rects || !f->depth_keys[0] ||
+                  !f->depth_keys[1] || !f->depth_order[0] || !f->depth_order[1]))
+        return false;
+    return true;
+}
+
+static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
+                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream) {
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    if (!img || !img->rgb || !frame_ok(f, g->count)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    const ScratchLayout L = ScratchLayout::make(g->count, f->instance_capacity);
+    if (f->scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
+    configure_once();
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* base = (unsigned char*)f->scratch;
+    Control* ctrl = (Control*)(base + L.control_off);
+    unsigned long long* proj_lb = (unsigned long long*)(base + L.proj_lb_off);
+    unsigned long long* emit_lb = (unsigned long long*)(base + L.emit_lb_off);
+    unsigned int* depth_lb = (unsigned int*)(base + L.depth_lb_off);
+    unsigned int* tile_lb = (unsigned int*)(base + L.tile_lb_off);
+    const int tiles_x = (cam->width + kTile - 1) / kTile;
+    const long long tiles = (long long)tiles_x * ((cam->height + kTile - 1) / kTile);
+    const int sms = device_sm_count();
+    if (ev) cudaEventRecord(ev[0], s);
+    cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (g->count > 0) {
+        launch_project(*g, *cam, *opt, *f, ctrl, proj_lb, (int)L.proj_blocks, s);
+        if (ev) cudaEventRecord(ev[1], s);
+        launch_sort32(f->depth_keys[0], f->depth_order[0], f->depth_keys[1], f->depth_order[1], g->count,
+                      &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, 0, &ctrl->error_flags, sms, s);
+        launch_emit(*f, ctrl, emit_lb, (int)L.proj_blocks, tiles_x, s);
+    } else if (ev) {
+        cudaEventRecord(ev[1], s);
+    }
+    launch_sort32(f->keys[0], f->vals[0], f->keys[1], f->vals[1], f->instance_capacity, &ctrl->tile_sort, tile_lb,
+                  L.sort_tiles, f->ranges, 2 * tiles, &ctrl->error_flags, sms, s);
+    if (ev) cudaEventRecord(ev[2], s);
+    launch_ranges(*f, ctrl, tiles, sms, s);
+    if (ev) cudaEventRecord(ev[3], s);
+    launch_composite(*f, ctrl, *cam, *opt, *img, s);
+    if (ev) cudaEventRecord(ev[4], s);
+    e = cudaGetLastError();
+    return map_cuda(e);
+}
+
 }  // namespace lumen
 
 using namespace lumen;
+
+struct LumenGpuStageTimer {
+    int max_frames = 0;
+    int next = 0;
+    cudaEvent_t* ev = nullptr;   /* max_frames x 5 */
+};
 
 extern "C" {
 
@@ -96,27 +158,39 @@ size_t lumen_gpu_scratch_bytes(int64_t n_gaussians, int64_t instance_capacity, i
     return ScratchLayout::make(n_gaussians, instance_capacity).total;
 }
 
-}  // extern "C"
-
-struct LumenGpuStageTimer {
-    int max_frames = 0;
-    int next = 0;
-    cudaEvent_t* ev = nullptr;   /* max_frames x 5 */
-};
-
-namespace lumen {
-
-static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
-                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream);
-
-}  // namespace lumen
-
-extern "C" {
-
 LumenStatus lumen_gpu_render_forward(const LumenGpuGaussians* g, const LumenViewCamera* cam,
                                      const LumenRenderOptions* opt, LumenGpuFrame* f, LumenGpuImage* img,
                                      void* stream) {
     return forward_impl(g, cam, opt, f, img, nullptr, stream);
+}
+
+LumenStatus lumen_gpu_read_counts(const LumenGpuFrame* f, LumenGpuCounts* c, void* stream) {
+    if (!f || !c || !f->scratch) return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    Control h;
+    cudaError_t e = cudaMemcpyAsync(&h, f->scratch, sizeof(Control), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return map_cuda(e);
+    c->n_visible = h.n_visible;
+    c->n_instances = (int64_t)h.n_instances;
+    c->error_flags = h.error_flags;
+    c->sorted_buffer = h.tile_sort.sorted_buffer;
+    c->varying_digits = (h.tile_sort.varying & 0xFFu) | ((h.depth_sort.varying & 0xFFu) << 8);
+    c->touched_tiles = h.touched_tiles;
+    c->depth_sorted_buffer = h.depth_sort.sorted_buffer;
+    c->reserved = 0;
+    return LUMEN_SUCCESS;
+}
+
+LumenStatus lumen_gpu_frame_sorted_keys64(const LumenGpuFrame* f, const LumenRenderOptions* opt, uint64_t* out,
+                                          void* stream) {
+    if (!f || !opt || !out || !f->scratch) return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    launch_sorted_keys64(*f, (const Control*)f->scratch, opt->key_mode, reinterpret_cast<unsigned long long*>(out),
+                         device_sm_count(), s);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return map_cuda(e);
 }
 
 LumenGpuStageTimer* lumen_gpu_stage_timer_create(int max_frames) {
@@ -170,61 +244,34 @@ LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* t, float stage_ms[4],
     return LUMEN_SUCCESS;
 }
 
-}  // extern "C"
-
-namespace lumen {
-
-static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
-                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream) {
-    LumenStatus st = check_inputs(g, cam, opt);
-    if (st != LUMEN_SUCCESS) return st;
-    if (!f || !img || !img->rgb || !f->scratch || !f->ranges || f->instance_capacity <= 0 ||
-        f->instance_capacity >= (1ll << 30) || !f->keys[0] || !f->keys[1] || !f->vals[0] || !f->vals[1])
-        return LUMEN_ERROR_INVALID_ARGUMENT;
-    if (g->count > 0 && (!f->records || !f->visible_ids || !f->radii)) return LUMEN_ERROR_INVALID_ARGUMENT;
-    const ScratchLayout L = ScratchLayout::make(g->count, f->instance_capacity);
-    if (f->scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
+LumenStatus lumen_gpu_sort_pairs(uint64_t* keys0, uint32_t* vals0, uint64_t* keys1, uint32_t* vals1, int64_t n,
+                                 void* scratch, size_t scratch_bytes, uint32_t* sorted_buffer, void* stream) {
+    if (n < 0 || n >= (1ll << 30) || !sorted_buffer) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (n > 0 && (!keys0 || !vals0 || !keys1 || !vals1 || !scratch)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    *sorted_buffer = 0;
+    if (n == 0) return LUMEN_SUCCESS;
+    const ScratchLayout L = ScratchLayout::make(0, n);
+    if (scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
     configure_once();
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* base = (unsigned char*)f->scratch;
+    unsigned char* base = (unsigned char*)scratch;
     Control* ctrl = (Control*)(base + L.control_off);
-    unsigned long long* plb = (unsigned long long*)(base + L.proj_lb_off);
-    unsigned int* slb = (unsigned int*)(base + L.sort_lb_off);
-    if (ev) cudaEventRecord(ev[0], s);
     cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
     if (e != cudaSuccess) return map_cuda(e);
-    if (g->count > 0) launch_project_emit(*g, *cam, *opt, *f, ctrl, plb, (int)L.proj_blocks, s);
-    if (ev) cudaEventRecord(ev[1], s);
-    const long long tiles = (long long)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
     const int sms = device_sm_count();
-    launch_sort(*f, ctrl, slb, L.sort_tiles, 2 * tiles, sms, s);
-    if (ev) cudaEventRecord(ev[2], s);
-    launch_ranges(*f, ctrl, tiles, sms, s);
-    if (ev) cudaEventRecord(ev[3], s);
-    launch_composite(*f, ctrl, *cam, *opt, *img, s);
-    if (ev) cudaEventRecord(ev[4], s);
-    e = cudaGetLastError();
-    return map_cuda(e);
-}
-
-}  // namespace lumen
-
-extern "C" {
-
-LumenStatus lumen_gpu_read_counts(const LumenGpuFrame* f, LumenGpuCounts* c, void* stream) {
-    if (!f || !c || !f->scratch) return LUMEN_ERROR_INVALID_ARGUMENT;
-    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long* k0 = reinterpret_cast<unsigned long long*>(keys0);
+    unsigned long long* k1 = reinterpret_cast<unsigned long long*>(keys1);
+    launch_key_stats64(k0, n, &ctrl->tile_sort, sms, s);
+    /* the tile-sort look-back region holds 8 digits x tiles x 256 entries */
+    launch_sort64(k0, vals0, k1, vals1, n, &ctrl->tile_sort, (unsigned int*)(base + L.tile_lb_off), L.sort_tiles,
+                  &ctrl->error_flags, sms, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return map_cuda(e);
     Control h;
-    cudaError_t e = cudaMemcpyAsync(&h, f->scratch, offsetof(Control, hist), cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(&h, ctrl, sizeof(Control), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return map_cuda(e);
-    c->n_visible = h.n_visible;
-    c->n_instances = (int64_t)h.n_instances;
-    c->error_flags = h.error_flags;
-    c->sorted_buffer = h.sorted_buffer;
-    c->varying_digits = h.varying_digits;
-    c->touched_tiles = h.touched_tiles;
-    return LUMEN_SUCCESS;
+    *sorted_buffer = h.tile_sort.sorted_buffer;
+    return status_from_flags(h.error_flags);
 }
 
 }  // extern "C"
@@ -241,10 +288,17 @@ struct LumenGpuRenderer {
 
 namespace {
 
+void free_per_gaussian(LumenGpuFrame& f) {
+    cudaFree(f.records); cudaFree(f.visible_ids); cudaFree(f.radii); cudaFree(f.rects);
+    for (int b = 0; b < 2; ++b) { cudaFree(f.depth_keys[b]); cudaFree(f.depth_order[b]); }
+    f.records = nullptr; f.visible_ids = nullptr; f.radii = nullptr; f.rects = nullptr;
+    for (int b = 0; b < 2; ++b) { f.depth_keys[b] = nullptr; f.depth_order[b] = nullptr; }
+}
+
 void free_frame(LumenGpuRenderer* r) {
     LumenGpuFrame& f = r->frame;
-    cudaFree(f.records); cudaFree(f.visible_ids); cudaFree(f.radii);
-    cudaFree(f.keys[0]); cudaFree(f.keys[1]); cudaFree(f.vals[0]); cudaFree(f.vals[1]);
+    free_per_gaussian(f);
+    for (int b = 0; b < 2; ++b) { cudaFree(f.keys[b]); cudaFree(f.vals[b]); }
     cudaFree(f.ranges); cudaFree(f.scratch);
     std::memset(&f, 0, sizeof(f));
     r->n_cap = r->tiles_cap = r->k_cap = 0;
@@ -255,13 +309,17 @@ LumenStatus ensure(LumenGpuRenderer* r, int64_t n, int64_t tiles, int64_t k) {
     LumenGpuFrame& f = r->frame;
     cudaError_t e = cudaSuccess;
     if (n > r->n_cap) {
-        int64_t nn = n + n / 8 + 1024;
-        cudaFree(f.records); cudaFree(f.visible_ids); cudaFree(f.radii);
-        f.records = nullptr; f.visible_ids = nullptr; f.radii = nullptr;
+        const int64_t nn = n + n / 8 + 1024;
+        free_per_gaussian(f);
         r->n_cap = 0;
         if ((e = cudaMalloc(&f.records, nn * sizeof(LumenSplatRecord))) != cudaSuccess) return map_cuda(e);
         if ((e = cudaMalloc(&f.visible_ids, nn * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
         if ((e = cudaMalloc(&f.radii, nn * sizeof(int32_t))) != cudaSuccess) return map_cuda(e);
+        if ((e = cudaMalloc(&f.rects, nn * sizeof(uint64_t))) != cudaSuccess) return map_cuda(e);
+        for (int b = 0; b < 2; ++b) {
+            if ((e = cudaMalloc(&f.depth_keys[b], nn * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
+            if ((e = cudaMalloc(&f.depth_order[b], nn * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
+        }
         r->n_cap = nn;
     }
     if (tiles > r->tiles_cap) {
@@ -282,7 +340,7 @@ LumenStatus ensure(LumenGpuRenderer* r, int64_t n, int64_t tiles, int64_t k) {
         r->k_cap = 0;
         f.instance_capacity = 0;
         for (int b = 0; b < 2; ++b) {
-            if ((e = cudaMalloc(&f.keys[b], kk * sizeof(uint64_t))) != cudaSuccess) return map_cuda(e);
+            if ((e = cudaMalloc(&f.keys[b], kk * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
             if ((e = cudaMalloc(&f.vals[b], kk * sizeof(uint32_t))) != cudaSuccess) return map_cuda(e);
         }
         r->k_cap = kk;
@@ -326,10 +384,11 @@ LumenStatus lumen_gpu_renderer_render(LumenGpuRenderer* r, const LumenGpuGaussia
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
     const int64_t tiles = (int64_t)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
-    int64_t k_guess = r->k_cap > 0 ? r->k_cap : (g->count * 8 > (1 << 20) ? g->count * 8 : (1 << 20));
+    const int64_t k_guess = r->k_cap > 0 ? r->k_cap : (g->count * 8 > (1 << 20) ? g->count * 8 : (1 << 20));
     st = ensure(r, g->count > 0 ? g->count : 1, tiles, k_guess);
     if (st != LUMEN_SUCCESS) return st;
     LumenGpuCounts c;
+    std::memset(&c, 0, sizeof(c));
     for (int attempt = 0; attempt < 2; ++attempt) {
         st = lumen_gpu_render_forward(g, cam, opt, &r->frame, img, stream);
         if (st != LUMEN_SUCCESS) return st;
@@ -340,36 +399,6 @@ LumenStatus lumen_gpu_renderer_render(LumenGpuRenderer* r, const LumenGpuGaussia
         if (st != LUMEN_SUCCESS) return st;
     }
     if (counts) *counts = c;
-    return status_from_flags(c.error_flags);
-}
-
-LumenStatus lumen_gpu_sort_pairs(uint64_t* keys0, uint32_t* vals0, uint64_t* keys1, uint32_t* vals1, int64_t n,
-                                 void* scratch, size_t scratch_bytes, uint32_t* sorted_buffer, void* stream) {
-    if (n < 0 || n >= (1ll << 30) || !sorted_buffer) return LUMEN_ERROR_INVALID_ARGUMENT;
-    if (n > 0 && (!keys0 || !vals0 || !keys1 || !vals1 || !scratch)) return LUMEN_ERROR_INVALID_ARGUMENT;
-    *sorted_buffer = 0;
-    if (n == 0) return LUMEN_SUCCESS;
-    const ScratchLayout L = ScratchLayout::make(0, n);
-    if (scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
-    configure_once();
-    cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* base = (unsigned char*)scratch;
-    Control* ctrl = (Control*)(base + L.control_off);
-    cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
-    if (e != cudaSuccess) return map_cuda(e);
-    LumenGpuFrame f;
-    std::memset(&f, 0, sizeof(f));
-    f.keys[0] = keys0; f.keys[1] = keys1; f.vals[0] = vals0; f.vals[1] = vals1;
-    f.instance_capacity = n;
-    const int sms = device_sm_count();
-    launch_key_stats(reinterpret_cast<const unsigned long long*>(keys0), n, ctrl, sms, s);
-    launch_sort(f, ctrl, (unsigned int*)(base + L.sort_lb_off), L.sort_tiles, 0, sms, s);
-    if ((e = cudaGetLastError()) != cudaSuccess) return map_cuda(e);
-    LumenGpuCounts c;
-    const LumenGpuFrame fs = f_scratch_only(scratch, scratch_bytes);
-    LumenStatus st = lumen_gpu_read_counts(&fs, &c, stream);
-    if (st != LUMEN_SUCCESS) return st;
-    *sorted_buffer = c.sorted_buffer;
     return status_from_flags(c.error_flags);
 }
 

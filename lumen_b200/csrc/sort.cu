@@ -1,67 +1,66 @@
 /*
- * sort.cu - K3/K4: stable LSD radix sort of the (tile << 32 | depth) keys
- * with their visible-index values, and the per-tile ranges.
+ * sort.cu - stable LSD radix sort of (key, value) pairs on the device, and
+ * the per-tile ranges.
  *
  * Reference: radix_sort_64bit, src/raster/radix_sort.mojo:39-87 (eight
  * stable 8-bit LSD passes with 256 buckets), and
  * TileRangeIndex.build_from_sorted_keys, src/raster/binning.mojo:51-73.
  *
- * B200 design (onesweep, Adinets & Merrill 2022):
+ * B200 design (onesweep, Adinets & Merrill 2022), for 32- or 64-bit keys:
  *  - one histogram pass reads the keys once and counts every digit that
- *    varies; a digit is constant when no key differs in that byte (the OR of
- *    all keys and the OR of all complemented keys, gathered during emission,
- *    tell which). Constant digits leave a stable sort unchanged, so their
- *    passes are skipped on the device; at 1080p with millimetre keys only 4
- *    of the 8 bytes vary.
+ *    varies. A digit is constant when no two keys differ in that byte (the
+ *    OR of all keys and the OR of all complemented keys, gathered by the
+ *    kernel that produced them, tell which); a pass over a constant digit
+ *    leaves a stable sort unchanged, so it is skipped on the device.
  *  - each digit pass is one persistent kernel: a CTA takes 4096-key tiles in
  *    ticket order, ranks its keys with warp-level match_any multisplit over
  *    per-warp shared-memory histograms (stable: warp order, then item order,
- *    then lane order), publishes per-digit tile counts, and resolves global
- *    digit offsets by decoupled look-back over earlier tiles. Keys are
- *    reordered in shared memory and written out in digit runs (coalesced).
+ *    then lane order), publishes per-digit tile counts, and resolves the
+ *    global digit offsets by decoupled look-back over earlier tiles. Keys
+ *    are reordered in shared memory and written out in digit runs.
  *  - every wait on another CTA's descriptor is bounded.
- * Per pass and key: 12 B read + 12 B written.
+ * Per pass and pair: (sizeof key + 4) B read and written.
  */
 #include "splat_common.cuh"
 
 namespace lumen {
 
-__device__ __forceinline__ unsigned int varying_from(const Control* c) {
-    unsigned long long v = c->key_or & c->key_or_not;
+__device__ __forceinline__ unsigned int varying_digits(const SortControl* c, int nbytes) {
+    const unsigned long long v = c->key_or & c->key_or_not;
     unsigned int m = 0;
-#pragma unroll
-    for (int d = 0; d < 8; ++d)
+    for (int d = 0; d < nbytes; ++d)
         if ((v >> (8 * d)) & 0xFFull) m |= 1u << d;
     return m;
 }
 
-__device__ __forceinline__ long long effective_count(const Control* c, long long capacity) {
-    long long k = (long long)c->n_instances;
+__device__ __forceinline__ long long sort_count(const SortControl* c, long long capacity) {
+    const long long k = (long long)c->n;
     return k < capacity ? k : capacity;
 }
 
-/* Histogram of every varying digit; also clears the look-back regions the
- * digit passes will use and fills the tile ranges with -1. */
+/* Histogram of every varying digit; clears the look-back regions of the
+ * passes that will run; optionally fills the tile ranges with -1. */
+template <typename KeyT>
 __global__ void __launch_bounds__(256)
-sort_histogram_kernel(const unsigned long long* __restrict__ keys, long long capacity, Control* ctrl,
-                      unsigned int* sort_lb, long long lb_tiles_cap, int* ranges, long long n_range_ints) {
-    __shared__ unsigned int h[8][256];
+histogram_kernel(const KeyT* __restrict__ keys, long long capacity, SortControl* sc, unsigned int* lb,
+                 long long lb_tiles_cap, int* ranges, long long n_range_ints) {
+    constexpr int kBytes = (int)sizeof(KeyT);
+    __shared__ unsigned int h[kBytes][256];
     const int tid = threadIdx.x, lane = tid & 31;
-    const long long K = effective_count(ctrl, capacity);
-    unsigned int varying = K > 1 ? varying_from(ctrl) : 0u;
-    for (int j = tid; j < 8 * 256; j += 256) (&h[0][0])[j] = 0u;
+    const long long K = sort_count(sc, capacity);
+    const unsigned int varying = K > 1 ? varying_digits(sc, kBytes) : 0u;
+    for (int j = tid; j < kBytes * 256; j += 256) (&h[0][0])[j] = 0u;
     __syncthreads();
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     const long long gtid = (long long)blockIdx.x * blockDim.x + tid;
     if (varying) {
         /* warps iterate in lockstep so match_any sees full warps */
-        const long long warp_base = gtid - lane;
-        for (long long base = warp_base; base < K; base += nthreads) {
+        for (long long base = gtid - lane; base < K; base += nthreads) {
             const long long i = base + lane;
             const bool valid = i < K;
-            const unsigned long long k = valid ? keys[i] : 0ull;
+            const KeyT k = valid ? keys[i] : (KeyT)0;
 #pragma unroll
-            for (int d = 0; d < 8; ++d) {
+            for (int d = 0; d < kBytes; ++d) {
                 if (!(varying & (1u << d))) continue;
                 const unsigned int b = valid ? (unsigned int)((k >> (8 * d)) & 0xFF) : (0x100u + lane);
                 const unsigned int peers = __match_any_sync(0xffffffffu, b);
@@ -71,28 +70,29 @@ sort_histogram_kernel(const unsigned long long* __restrict__ keys, long long cap
     }
     __syncthreads();
     if (varying) {
-        for (int j = tid; j < 8 * 256; j += 256) {
+        for (int j = tid; j < kBytes * 256; j += 256) {
             const int d = j >> 8;
             const unsigned int c = (&h[0][0])[j];
-            if ((varying & (1u << d)) && c) atomicAdd(&ctrl->hist[d][j & 255], c);
+            if ((varying & (1u << d)) && c) atomicAdd(&sc->hist[d][j & 255], c);
         }
         const long long tiles = (K + kSortTile - 1) / kSortTile;
-        for (int d = 0; d < 8; ++d) {
+        for (int d = 0; d < kBytes; ++d) {
             if (!(varying & (1u << d))) continue;
-            unsigned int* region = sort_lb + (size_t)d * (size_t)lb_tiles_cap * 256;
+            unsigned int* region = lb + (size_t)d * (size_t)lb_tiles_cap * 256;
             for (long long j = gtid; j < tiles * 256; j += nthreads) region[j] = 0u;
         }
     }
     if (ranges)
         for (long long j = gtid; j < n_range_ints; j += nthreads) ranges[j] = -1;
     if (blockIdx.x == 0 && tid == 0) {
-        ctrl->varying_digits = varying;
-        ctrl->sorted_buffer = (unsigned int)(__popc(varying) & 1);
+        sc->varying = varying;
+        sc->sorted_buffer = (unsigned int)(__popc(varying) & 1);
     }
 }
 
+template <typename KeyT>
 struct PassSmem {
-    unsigned long long keys[kSortTile];
+    KeyT keys[kSortTile];
     unsigned int vals[kSortTile];
     unsigned int whist[kSortThreads / 32][256];
     unsigned int digit_start[256];
@@ -102,8 +102,8 @@ struct PassSmem {
     unsigned int tile;
 };
 
-/* Sum over earlier tiles of digit `t`'s count, by walking back until a tile
- * with an inclusive prefix is found. */
+/* Sum over earlier tiles of digit t's count, walking back until a tile with
+ * an inclusive prefix is found. */
 __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, int tile, int t, unsigned int* err) {
     unsigned int excl = 0;
     for (int j = tile - 1; j >= 0; --j) {
@@ -125,27 +125,28 @@ __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, i
     return excl;
 }
 
-__global__ void __launch_bounds__(kSortThreads)
-onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigned int* sort_lb,
-                     long long lb_tiles_cap, int digit) {
+template <typename KeyT>
+__global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? 3 : 2)
+onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
+                     unsigned int* lb_all, long long lb_tiles_cap, unsigned int* err, int digit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    PassSmem& s = *reinterpret_cast<PassSmem*>(smem_raw);
-    const unsigned int varying = ctrl->varying_digits;
+    PassSmem<KeyT>& s = *reinterpret_cast<PassSmem<KeyT>*>(smem_raw);
+    const unsigned int varying = sc->varying;
     if (!(varying & (1u << digit))) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int src = __popc(varying & ((1u << digit) - 1u)) & 1;
-    const unsigned long long* __restrict__ kin = reinterpret_cast<const unsigned long long*>(src ? f.keys[1] : f.keys[0]);
-    const unsigned int* __restrict__ vin = src ? f.vals[1] : f.vals[0];
-    unsigned long long* __restrict__ kout = reinterpret_cast<unsigned long long*>(src ? f.keys[0] : f.keys[1]);
-    unsigned int* __restrict__ vout = src ? f.vals[0] : f.vals[1];
-    const long long K = effective_count(ctrl, capacity);
+    const KeyT* __restrict__ kin = src ? k1 : k0;
+    const unsigned int* __restrict__ vin = src ? v1 : v0;
+    KeyT* __restrict__ kout = src ? k0 : k1;
+    unsigned int* __restrict__ vout = src ? v0 : v1;
+    const long long K = sort_count(sc, capacity);
     const long long ntiles = (K + kSortTile - 1) / kSortTile;
     const int shift = 8 * digit;
-    unsigned int* lb = sort_lb + (size_t)digit * (size_t)lb_tiles_cap * 256;
+    unsigned int* lb = lb_all + (size_t)digit * (size_t)lb_tiles_cap * 256;
 
     /* global exclusive offsets of this digit's buckets */
     {
-        const unsigned int c = ctrl->hist[digit][tid];
+        const unsigned int c = sc->hist[digit][tid];
         unsigned int x = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -161,33 +162,32 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
     }
 
     for (;;) {
-        if (tid == 0) s.tile = atomicAdd(&ctrl->pass_ticket[digit], 1u);
+        if (tid == 0) s.tile = atomicAdd(&sc->pass_ticket[digit], 1u);
         __syncthreads();
         const long long tile = s.tile;
         if (tile >= ntiles) break;
         const long long base = tile * kSortTile;
 
-        /* load: warp w owns keys [base + w*512, +512), item i of lane l is base + w*512 + i*32 + l */
-        unsigned long long k[kSortItems];
+        /* warp w owns keys [base + w*512, +512); item i of lane l is base + w*512 + i*32 + l */
+        KeyT k[kSortItems];
         unsigned int v[kSortItems];
-        unsigned int dig[kSortItems];
         unsigned short rank[kSortItems];
 #pragma unroll
         for (int it = 0; it < kSortItems; ++it) {
             const long long idx = base + warp * (kSortItems * 32) + it * 32 + lane;
             const bool valid = idx < K;
-            k[it] = valid ? kin[idx] : 0ull;
+            k[it] = valid ? kin[idx] : (KeyT)0;
             v[it] = valid ? vin[idx] : 0u;
-            dig[it] = valid ? (unsigned int)((k[it] >> shift) & 0xFF) : (0x100u + lane);
         }
+        const long long wbase = base + warp * (kSortItems * 32);
         for (int b = lane; b < 256; b += 32) s.whist[warp][b] = 0u;
         __syncwarp();
         /* warp-level stable multisplit */
 #pragma unroll
         for (int it = 0; it < kSortItems; ++it) {
-            const unsigned int d = dig[it];
+            const bool valid = wbase + it * 32 + lane < K;
+            const unsigned int d = valid ? (unsigned int)((k[it] >> shift) & 0xFF) : (0x100u + lane);
             const unsigned int peers = __match_any_sync(0xffffffffu, d);
-            const bool valid = d < 256u;
             unsigned int prior = 0;
             if (valid) prior = s.whist[warp][d];
             __syncwarp();
@@ -196,7 +196,7 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
             rank[it] = (unsigned short)(prior + __popc(peers & lanemask_lt()));
         }
         __syncthreads();
-        /* per digit t: warp-exclusive offsets and the tile's count */
+        /* digit t: warp-exclusive offsets and the tile's count */
         const int t = tid;
         unsigned int run = 0;
 #pragma unroll
@@ -207,7 +207,6 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
         }
         const unsigned int count = run;
         st_volatile_u32(lb + (size_t)tile * 256 + t, (tile == 0 ? kDescIncl32 : kDescAgg32) | count);
-        /* block exclusive scan of the digit counts */
         {
             unsigned int x = count;
 #pragma unroll
@@ -223,7 +222,7 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
         }
         unsigned int excl = 0;
         if (tile > 0) {
-            excl = lookback_digit(lb, (int)tile, t, &ctrl->error_flags);
+            excl = lookback_digit(lb, (int)tile, t, err);
             st_volatile_u32(lb + (size_t)tile * 256 + t, kDescIncl32 | (excl + count));
         }
         s.gbase[t] = (long long)s.goffset[t] + (long long)excl - (long long)s.digit_start[t];
@@ -231,8 +230,8 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
         /* reorder through shared memory */
 #pragma unroll
         for (int it = 0; it < kSortItems; ++it) {
-            const unsigned int d = dig[it];
-            if (d < 256u) {
+            if (wbase + it * 32 + lane < K) {
+                const unsigned int d = (unsigned int)((k[it] >> shift) & 0xFF);
                 const unsigned int pos = s.digit_start[d] + s.whist[warp][d] + rank[it];
                 s.keys[pos] = k[it];
                 s.vals[pos] = v[it];
@@ -241,7 +240,7 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
         __syncthreads();
         const int nvalid = (int)((K - base) < kSortTile ? (K - base) : kSortTile);
         for (int j = tid; j < nvalid; j += kSortThreads) {
-            const unsigned long long kk = s.keys[j];
+            const KeyT kk = s.keys[j];
             const unsigned int d = (unsigned int)((kk >> shift) & 0xFF);
             const long long out = s.gbase[d] + j;
             kout[out] = kk;
@@ -251,55 +250,42 @@ onesweep_pass_kernel(LumenGpuFrame f, long long capacity, Control* ctrl, unsigne
     }
 }
 
-/* binning.mojo:51-73 in parallel: a tile's range starts where its id first
- * appears in the sorted keys and ends after it last appears. Ranges were
- * filled with -1 by the histogram kernel (empty tiles stay (-1, -1)). */
+/* binning.mojo:51-73 in parallel, on tile-sorted 32-bit tile ids: a tile's
+ * range starts where its id first appears and ends after it last appears.
+ * Empty tiles keep the (-1, -1) the histogram kernel wrote. */
 __global__ void __launch_bounds__(256)
-tile_ranges_kernel(LumenGpuFrame f, long long capacity, long long n_tiles, Control* ctrl) {
-    const long long K = effective_count(ctrl, capacity);
-    const unsigned long long* __restrict__ keys = reinterpret_cast<const unsigned long long*>(ctrl->sorted_buffer ? f.keys[1] : f.keys[0]);
+tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, long long n_tiles,
+                   int* ranges, Control* ctrl) {
+    const SortControl* sc = &ctrl->tile_sort;
+    const long long K = sort_count(sc, capacity);
+    const unsigned int* __restrict__ keys = sc->sorted_buffer ? k1 : k0;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     unsigned int touched = 0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < K; i += nthreads) {
-        const unsigned int t = (unsigned int)(keys[i] >> 32);
+        const unsigned int t = keys[i];
         if ((long long)t >= n_tiles) {   /* self-check: a tile id outside the grid */
             atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
             continue;
         }
-        const bool first = i == 0 || (unsigned int)(keys[i - 1] >> 32) != t;
-        const bool last = i == K - 1 || (unsigned int)(keys[i + 1] >> 32) != t;
-        if (first) { f.ranges[2 * (size_t)t] = (int)i; ++touched; }
-        if (last) f.ranges[2 * (size_t)t + 1] = (int)(i + 1);
+        const bool first = i == 0 || keys[i - 1] != t;
+        const bool last = i == K - 1 || keys[i + 1] != t;
+        if (first) { ranges[2 * (size_t)t] = (int)i; ++touched; }
+        if (last) ranges[2 * (size_t)t + 1] = (int)(i + 1);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) touched += __shfl_xor_sync(0xffffffffu, touched, o);
     if ((threadIdx.x & 31) == 0 && touched) atomicAdd(&ctrl->touched_tiles, touched);
 }
 
-size_t onesweep_smem_bytes() { return sizeof(PassSmem); }
-
-void launch_sort(LumenGpuFrame& f, Control* ctrl, unsigned int* sort_lb, long long lb_tiles_cap,
-                 long long n_range_ints, int num_sms, cudaStream_t st) {
-    const long long cap = (long long)f.instance_capacity;
-    sort_histogram_kernel<<<num_sms * 4, 256, 0, st>>>(reinterpret_cast<const unsigned long long*>(f.keys[0]), cap, ctrl, sort_lb, lb_tiles_cap, f.ranges,
-                                                       n_range_ints);
-    const size_t smem = sizeof(PassSmem);
-    for (int d = 0; d < 8; ++d)
-        onesweep_pass_kernel<<<num_sms * 2, kSortThreads, smem, st>>>(f, cap, ctrl, sort_lb, lb_tiles_cap, d);
-}
-
-void launch_ranges(LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st) {
-    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f, (long long)f.instance_capacity, n_tiles, ctrl);
-}
-
-/* OR and OR-of-complement of n keys, for a sort whose keys were not emitted
- * by project_emit (lumen_gpu_sort_pairs). */
+/* OR and OR-of-complement of n keys and the pair count, for sorts whose
+ * keys come from the caller (lumen_gpu_sort_pairs). */
+template <typename KeyT>
 __global__ void __launch_bounds__(256)
-key_stats_kernel(const unsigned long long* __restrict__ keys, long long n, Control* ctrl) {
+key_stats_kernel(const KeyT* __restrict__ keys, long long n, SortControl* sc) {
     unsigned long long o = 0ull, no = 0ull;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += nthreads) {
-        const unsigned long long k = keys[i];
+        const unsigned long long k = (unsigned long long)keys[i];
         o |= k;
         no |= ~k;
     }
@@ -309,18 +295,74 @@ key_stats_kernel(const unsigned long long* __restrict__ keys, long long n, Contr
         no |= __shfl_xor_sync(0xffffffffu, no, off);
     }
     if ((threadIdx.x & 31) == 0) {
-        atomicOr(&ctrl->key_or, o);
-        atomicOr(&ctrl->key_or_not, no);
+        atomicOr(&sc->key_or, o);
+        atomicOr(&sc->key_or_not, no);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->n_instances = (unsigned long long)n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->n = (unsigned long long)n;
 }
 
-void launch_key_stats(const unsigned long long* keys, long long n, Control* ctrl, int num_sms, cudaStream_t st) {
-    key_stats_kernel<<<num_sms * 2, 256, 0, st>>>(keys, n, ctrl);
+/* Rebuild the reference's 64-bit keys: (tile << 32) | depth key of the
+ * instance's splat. */
+__global__ void sorted_keys64_kernel(const unsigned int* k0, const unsigned int* k1, const unsigned int* v0,
+                                     const unsigned int* v1, const LumenSplatRecord* records, long long capacity,
+                                     int key_mode, const Control* ctrl, unsigned long long* out) {
+    const SortControl* sc = &ctrl->tile_sort;
+    const long long K = sort_count(sc, capacity);
+    const unsigned int* keys = sc->sorted_buffer ? k1 : k0;
+    const unsigned int* vals = sc->sorted_buffer ? v1 : v0;
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < K; i += nthreads) {
+        const unsigned int v = vals[i];
+        out[i] = ((unsigned long long)keys[i] << 32) | depth_key(records[v].depth, key_mode);
+    }
+}
+
+template <typename KeyT>
+void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
+                      unsigned int* lb, long long lb_tiles_cap, int* ranges, long long n_range_ints,
+                      unsigned int* err, int num_sms, cudaStream_t st) {
+    histogram_kernel<KeyT><<<num_sms * 4, 256, 0, st>>>(k0, capacity, sc, lb, lb_tiles_cap, ranges, n_range_ints);
+    const size_t smem = sizeof(PassSmem<KeyT>);
+    const int ctas_per_sm = sizeof(KeyT) == 4 ? 3 : 2;   /* matches __launch_bounds__: all CTAs resident */
+    for (int d = 0; d < (int)sizeof(KeyT); ++d)
+        onesweep_pass_kernel<KeyT><<<num_sms * ctas_per_sm, kSortThreads, smem, st>>>(k0, v0, k1, v1, capacity,
+                                                                                       sc, lb, lb_tiles_cap, err, d);
+}
+
+void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
+                   SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges, long long n_range_ints,
+                   unsigned int* err, int num_sms, cudaStream_t st) {
+    launch_sort_impl<unsigned int>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_ints, err,
+                                   num_sms, st);
+}
+
+void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
+                   long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
+                   int num_sms, cudaStream_t st) {
+    launch_sort_impl<unsigned long long>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, 0, err, num_sms,
+                                         st);
+}
+
+void launch_ranges(const LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st) {
+    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f.keys[0], f.keys[1], (long long)f.instance_capacity, n_tiles,
+                                                    f.ranges, ctrl);
+}
+
+void launch_key_stats64(const unsigned long long* keys, long long n, SortControl* sc, int num_sms, cudaStream_t st) {
+    key_stats_kernel<unsigned long long><<<num_sms * 2, 256, 0, st>>>(keys, n, sc);
+}
+
+void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_mode, unsigned long long* out,
+                          int num_sms, cudaStream_t st) {
+    sorted_keys64_kernel<<<num_sms * 4, 256, 0, st>>>(f.keys[0], f.keys[1], f.vals[0], f.vals[1], f.records,
+                                                      (long long)f.instance_capacity, key_mode, ctrl, out);
 }
 
 void configure_sort_kernels() {
-    cudaFuncSetAttribute(onesweep_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PassSmem));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned int>));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned long long>));
 }
 
 }  // namespace lumen

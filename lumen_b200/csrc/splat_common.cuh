@@ -24,26 +24,34 @@ namespace lumen {
 constexpr int kTile = 16;
 constexpr int kTilePixels = 256;
 
+/* State of one stable radix sort of (key, value) pairs. The producer of the
+ * keys fills n and the OR / OR-of-complement of all keys; a digit (byte)
+ * varies iff some key has a 1 and some key a 0 in it, and only varying
+ * digits get a pass. */
+struct SortControl {
+    unsigned long long n;                /* pairs to sort */
+    unsigned long long key_or;
+    unsigned long long key_or_not;
+    unsigned int varying;                /* bit d: byte d varies */
+    unsigned int sorted_buffer;          /* 0 or 1: where the sorted pairs end */
+    unsigned int pass_ticket[8];         /* tile order of each digit pass */
+    unsigned int hist[8][256];           /* histograms of the varying digits */
+};
+
 /* Control block at the start of a frame's scratch. Zeroed by the host
  * before every frame (one cudaMemsetAsync), then owned by the kernels. */
 struct Control {
     unsigned long long n_instances;      /* K, even if above capacity */
-    unsigned long long key_or;           /* OR of all emitted keys */
-    unsigned long long key_or_not;       /* OR of ~key: a bit varies iff set in both */
     unsigned int n_visible;              /* V */
-    unsigned int proj_ticket;            /* block order for the project look-back */
+    unsigned int proj_ticket;            /* block order of the project look-back */
+    unsigned int emit_ticket;            /* block order of the emit look-back */
     unsigned int error_flags;            /* LUMEN_GPU_ERR_* */
-    unsigned int varying_digits;         /* bit d: byte d of the keys varies */
-    unsigned int sorted_buffer;          /* 0 or 1: where the sorted pairs end */
     unsigned int touched_tiles;
-    unsigned int pass_ticket[8];         /* tile order of each digit pass */
-    unsigned int hist_done;              /* blocks that finished the histogram */
-    unsigned int pad[7];
-    unsigned int hist[8][256];           /* digit histograms of the varying digits */
+    unsigned int pad[9];
+    SortControl depth_sort;              /* visible splats by depth key */
+    SortControl tile_sort;               /* instances by tile id */
 };
 
-/* Scratch layout: [Control][project look-back: 2 x u64 per block][sort
- * look-back: 8 digit passes x tiles x 256 digits x u32]. */
 constexpr int kProjThreads = 256;
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
@@ -51,22 +59,35 @@ constexpr int kSortTile = kSortThreads * kSortItems;   /* 4096 keys per tile */
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+/* Scratch layout: [Control][project look-back: u64 per block][emit
+ * look-back: u64 per block][depth-sort look-back: 4 passes x tiles x 256 x
+ * u32][tile-sort look-back: 8 passes x tiles x 256 x u32 (8 so that the
+ * standalone 64-bit pair sort can use it)]. */
 struct ScratchLayout {
-    size_t control_off, proj_lb_off, sort_lb_off, total;
-    int64_t proj_blocks, sort_tiles;
+    size_t control_off, proj_lb_off, emit_lb_off, depth_lb_off, tile_lb_off, total;
+    int64_t proj_blocks, depth_tiles, sort_tiles;
     __host__ __device__ static ScratchLayout make(int64_t n, int64_t capacity) {
         ScratchLayout L;
         L.proj_blocks = (n + kProjThreads - 1) / kProjThreads;
+        L.depth_tiles = (n + kSortTile - 1) / kSortTile;
         L.sort_tiles = (capacity + kSortTile - 1) / kSortTile;
         L.control_off = 0;
         L.proj_lb_off = align_up(sizeof(Control), 256);
-        L.sort_lb_off = align_up(L.proj_lb_off + (size_t)L.proj_blocks * 2 * sizeof(unsigned long long), 256);
-        L.total = align_up(L.sort_lb_off + (size_t)8 * (size_t)L.sort_tiles * 256 * sizeof(unsigned int), 256);
+        L.emit_lb_off = align_up(L.proj_lb_off + (size_t)L.proj_blocks * sizeof(unsigned long long), 256);
+        L.depth_lb_off = align_up(L.emit_lb_off + (size_t)L.proj_blocks * sizeof(unsigned long long), 256);
+        L.tile_lb_off = align_up(L.depth_lb_off + (size_t)4 * (size_t)L.depth_tiles * 256 * sizeof(unsigned int), 256);
+        L.total = align_up(L.tile_lb_off + (size_t)8 * (size_t)L.sort_tiles * 256 * sizeof(unsigned int), 256);
         return L;
     }
-    /* bytes the host must zero before a frame */
-    size_t zeroed_prefix() const { return sort_lb_off; }
+    /* bytes the host must zero before a frame (control and both scans) */
+    size_t zeroed_prefix() const { return depth_lb_off; }
 };
+
+/* Tile rectangle of a visible splat, 16 bits per bound. */
+__host__ __device__ inline unsigned long long pack_rect(int min_tx, int min_ty, int max_tx, int max_ty) {
+    return (unsigned long long)(unsigned short)min_tx | ((unsigned long long)(unsigned short)min_ty << 16) |
+           ((unsigned long long)(unsigned short)max_tx << 32) | ((unsigned long long)(unsigned short)max_ty << 48);
+}
 
 /* Bounded spin: after this many polls a wait gives up, sets
  * LUMEN_GPU_ERR_SPIN_TIMEOUT and continues with a zero contribution. */

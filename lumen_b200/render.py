@@ -31,12 +31,16 @@ def _stream_handle(device: torch.device) -> int:
 
 @dataclass
 class Frame:
-    """Work buffers of one frame (torch-owned device memory)."""
+    """Work buffers of one frame (torch-owned device memory); the layout of
+    LumenGpuFrame in include/lumen_gpu.h."""
     records: torch.Tensor       # [N, 12] float32 (48-byte records by visible index)
     visible_ids: torch.Tensor   # [N] int32 (Gaussian index of each record)
     radii: torch.Tensor         # [N] int32
-    keys: list                  # 2 x [cap] int64 (uint64 bits)
-    vals: list                  # 2 x [cap] int32 (uint32 bits)
+    rects: torch.Tensor         # [N] int64 packed tile rectangles
+    depth_keys: list            # 2 x [N] int32 (uint32 depth keys)
+    depth_order: list           # 2 x [N] int32 (visible indices in depth order)
+    keys: list                  # 2 x [cap] int32 (uint32 tile ids)
+    vals: list                  # 2 x [cap] int32 (uint32 visible indices)
     ranges: torch.Tensor        # [tiles, 2] int32
     scratch: torch.Tensor       # uint8
     capacity: int
@@ -47,10 +51,10 @@ class Frame:
         n1 = max(n, 1)
         scratch_bytes = int(lib.lumen_gpu_scratch_bytes(n1, capacity, tiles))
         kw = dict(device=device)
-        return Frame(torch.empty((n1, RECORD_FLOATS), dtype=torch.float32, **kw),
-                     torch.empty(n1, dtype=torch.int32, **kw), torch.empty(n1, dtype=torch.int32, **kw),
-                     [torch.empty(capacity, dtype=torch.int64, **kw) for _ in range(2)],
-                     [torch.empty(capacity, dtype=torch.int32, **kw) for _ in range(2)],
+        i32 = lambda m: torch.empty(m, dtype=torch.int32, **kw)
+        return Frame(torch.empty((n1, RECORD_FLOATS), dtype=torch.float32, **kw), i32(n1), i32(n1),
+                     torch.empty(n1, dtype=torch.int64, **kw), [i32(n1), i32(n1)], [i32(n1), i32(n1)],
+                     [i32(capacity), i32(capacity)], [i32(capacity), i32(capacity)],
                      torch.empty((tiles, 2), dtype=torch.int32, **kw),
                      torch.empty(scratch_bytes, dtype=torch.uint8, **kw), capacity)
 
@@ -60,6 +64,9 @@ class Frame:
     def c_struct(self) -> L.LumenGpuFrame:
         f = L.LumenGpuFrame()
         f.records, f.visible_ids, f.radii = _p(self.records), _p(self.visible_ids), _p(self.radii)
+        f.rects = _p(self.rects)
+        f.depth_keys[0], f.depth_keys[1] = _p(self.depth_keys[0]), _p(self.depth_keys[1])
+        f.depth_order[0], f.depth_order[1] = _p(self.depth_order[0]), _p(self.depth_order[1])
         f.keys[0], f.keys[1] = _p(self.keys[0]), _p(self.keys[1])
         f.vals[0], f.vals[1] = _p(self.vals[0]), _p(self.vals[1])
         f.instance_capacity = self.capacity
@@ -82,9 +89,22 @@ class RenderResult:
     varying_digits: int
     sorted_buffer: int
     frame: Frame
+    options: RenderOptions = None
 
     @property
     def sorted_keys(self) -> torch.Tensor:
+        """The reference's 64-bit keys (tile << 32 | depth key) in sorted
+        order, rebuilt on the device (int64 tensor holding uint64 bits)."""
+        lib = L.load()
+        out = torch.empty(max(self.n_instances, 1), dtype=torch.int64, device=self.rgb.device)
+        fs = self.frame.c_struct()
+        opt = L.render_options(self.options or RenderOptions())
+        L.check(lib.lumen_gpu_frame_sorted_keys64(C.byref(fs), C.byref(opt), _p(out),
+                                                  _stream_handle(self.rgb.device)), "sorted_keys64")
+        return out[: self.n_instances]
+
+    @property
+    def sorted_tiles(self) -> torch.Tensor:
         return self.frame.keys[self.sorted_buffer][: self.n_instances]
 
     @property
@@ -160,7 +180,8 @@ def render(means: torch.Tensor, scales: torch.Tensor, quats: torch.Tensor, opaci
                            f"render_forward device flags {counts.error_flags:#x}")
     _capacity_hint[key] = frame.capacity
     return RenderResult(rgb, depth, alpha, ncon, last, int(counts.n_visible), int(counts.n_instances),
-                        int(counts.touched_tiles), int(counts.varying_digits), int(counts.sorted_buffer), frame)
+                        int(counts.touched_tiles), int(counts.varying_digits), int(counts.sorted_buffer), frame,
+                        options)
 
 
 def sort_pairs(keys: torch.Tensor, vals: torch.Tensor):

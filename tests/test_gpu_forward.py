@@ -161,7 +161,8 @@ def test_medium_box_scene():
     s, op = sc.activated()
     cam = scenes.camera_config1(480, 270)
     g, o = run_both(sc.means, s, sc.quats, op, sc.sh, cam, RenderOptions())
-    assert g.varying_digits & ~0x33 & 0xFF == 0   # depth bytes 0-1 and tile bytes 4-5 only
+    # tile ids < 2^16 and millimetre depth keys 5000..11000: two digit passes per sort
+    assert g.varying_digits & 0xFF == 0x3 and (g.varying_digits >> 8) & 0xFF == 0x3
     assert_parity(g, o, check_image_bits=True)
 
 
