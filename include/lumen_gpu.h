@@ -204,6 +204,16 @@ LumenStatus lumen_gpu_render_forward_timed(const LumenGpuGaussians* gaussians, c
 LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms[4], float* total_ms,
                                        int* n_frames);
 
+/* The device camera lumen_rasterize uses for a look-at LumenCamera and a
+ * width x height frame: fx = fy = H / (2 tan(fov_y / 2)), principal point
+ * (W/2, H/2) (c_api/src/lumen_c.c:393-395,422-423), rotation with camera z
+ * toward the target, x right and y down ("up" is up in the image), near and
+ * far planes as given (lumen_rasterize passes the rasterizer config's). No
+ * counterpart in the reference, which builds an OpenGL view matrix inline
+ * (lumen_c.c:353-369,397). */
+LumenStatus lumen_gpu_camera_from_lookat(const LumenCamera* camera, uint32_t width, uint32_t height,
+                                         float near_plane, float far_plane, LumenViewCamera* out);
+
 /* Append n splats to a cloud in one copy. No counterpart in the reference:
  * the bulk form of lumen_cloud_add_gaussian (c_api/include/lumen.h:129),
  * with the same growth rule and error codes. */

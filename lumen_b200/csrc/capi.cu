@@ -414,16 +414,7 @@ LumenStatus lumen_rasterize(LumenRasterizer* r, const LumenCloud* cloud, const L
     if ((st = ensure_image(r, npix)) != LUMEN_SUCCESS) return st;
 
     LumenViewCamera cam;
-    std::memset(&cam, 0, sizeof(cam));
-    cam.position[0] = camera->position.x; cam.position[1] = camera->position.y; cam.position[2] = camera->position.z;
-    look_at_rotation(camera->position, camera->target, camera->up, cam.rotation);
-    const float fov_y = camera->fov_y_degrees * (float)M_PI / 180.0f;
-    const float fy = (float)H / (2.0f * tanf(fov_y * 0.5f));
-    cam.fx = fy; cam.fy = fy;
-    cam.cx = (float)W * 0.5f; cam.cy = (float)H * 0.5f;
-    cam.near_plane = r->config.near_plane;
-    cam.far_plane = r->config.far_plane;
-    cam.width = (int32_t)W; cam.height = (int32_t)H;
+    lumen_gpu_camera_from_lookat(camera, W, H, r->config.near_plane, r->config.far_plane, &cam);
 
     LumenRenderOptions opt;
     std::memset(&opt, 0, sizeof(opt));
@@ -473,6 +464,27 @@ LumenStatus lumen_rasterize(LumenRasterizer* r, const LumenCloud* cloud, const L
         stats->rasterize_time_ms = ms;
         stats->frames_per_second = ms > 0.001f ? 1000.0f / ms : 10000.0f;
     }
+    return LUMEN_SUCCESS;
+}
+
+LumenStatus lumen_gpu_camera_from_lookat(const LumenCamera* camera, uint32_t W, uint32_t H, float near_plane,
+                                         float far_plane, LumenViewCamera* cam) {
+    if (!camera || !cam || W == 0 || H == 0) return LUMEN_ERROR_INVALID_ARGUMENT;
+    std::memset(cam, 0, sizeof(*cam));
+    cam->position[0] = camera->position.x;
+    cam->position[1] = camera->position.y;
+    cam->position[2] = camera->position.z;
+    look_at_rotation(camera->position, camera->target, camera->up, cam->rotation);
+    const float fov_y = camera->fov_y_degrees * (float)M_PI / 180.0f;
+    const float fy = (float)H / (2.0f * tanf(fov_y * 0.5f));
+    cam->fx = fy;
+    cam->fy = fy;
+    cam->cx = (float)W * 0.5f;
+    cam->cy = (float)H * 0.5f;
+    cam->near_plane = near_plane;
+    cam->far_plane = far_plane;
+    cam->width = (int32_t)W;
+    cam->height = (int32_t)H;
     return LUMEN_SUCCESS;
 }
 
