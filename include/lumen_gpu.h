@@ -214,6 +214,21 @@ LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms
 LumenStatus lumen_gpu_camera_from_lookat(const LumenCamera* camera, uint32_t width, uint32_t height,
                                          float near_plane, float far_plane, LumenViewCamera* out);
 
+/* Stable in-place sort of n (uint64 key, uint32 value) pairs that allocates
+ * nothing. No counterpart in the reference. For callers that cannot call
+ * cudaMalloc: code inside a host application that owns all device memory
+ * (an engine plugin, an FFI host with its own allocator), or a frame loop
+ * that must not allocate because allocation can synchronise the device.
+ * The caller passes keys and vals (device memory) and gets them back sorted;
+ * the sort's own work memory is a static device array of the library sized
+ * for LUMEN_GPU_NOALLOC_MAX_PAIRS pairs (about 3.6 MB per GPU that loads the
+ * library, kept until exit). Larger n returns LUMEN_ERROR_INVALID_ARGUMENT.
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture). All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. Waits for `stream`. */
+#define LUMEN_GPU_NOALLOC_MAX_PAIRS 262144
+LumenStatus lumen_gpu_sort_pairs_noalloc(uint64_t* keys, uint32_t* vals, int64_t n, void* stream);
+
 /* Append n splats to a cloud in one copy. No counterpart in the reference:
  * the bulk form of lumen_cloud_add_gaussian (c_api/include/lumen.h:129),
  * with the same growth rule and error codes. */

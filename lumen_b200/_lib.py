@@ -147,6 +147,7 @@ SIGNATURES = {
     "lumen_gpu_frame_sorted_keys64": (C.c_int, [C.POINTER(LumenGpuFrame), C.POINTER(LumenRenderOptions), _P, _P]),
     "lumen_gpu_sort_pairs": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, C.c_size_t, C.POINTER(C.c_uint32), _P]),
     "lumen_cloud_append": (C.c_int, [_P, C.POINTER(LumenGaussian), C.c_size_t]),
+    "lumen_gpu_sort_pairs_noalloc": (C.c_int, [_P, _P, C.c_int64, _P]),
     "lumen_gpu_camera_from_lookat": (C.c_int, [C.POINTER(LumenCamera), C.c_uint32, C.c_uint32, C.c_float,
                                                C.c_float, C.POINTER(LumenViewCamera)]),
     "lumen_gpu_stage_timer_create": (_P, [C.c_int]),
