@@ -214,6 +214,45 @@ LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms
 LumenStatus lumen_gpu_camera_from_lookat(const LumenCamera* camera, uint32_t width, uint32_t height,
                                          float near_plane, float far_plane, LumenViewCamera* out);
 
+/* ------------------------------------------------------------- backward -- */
+
+/* Gradient outputs, device memory, same layouts as LumenGpuGaussians:
+ * means [N,3], scales [N,3], quats [N,4], opacities [N], sh [N,48]. When the
+ * forward ran with params_are_logits, scales and opacities receive the
+ * gradients of the log-scales and the opacity logits. splat2d is a work
+ * buffer of N x 10 floats (per-Gaussian gradients of the 2-D splat: centre,
+ * conic, opacity, colour, depth), zeroed by the call. */
+typedef struct {
+    float* means;
+    float* scales;
+    float* quats;
+    float* opacities;
+    float* sh;
+    float* splat2d;
+} LumenGpuGradients;
+
+/* Gradients of a scalar loss L through the forward that filled `frame`
+ * (same gaussians, camera and options; the frame must not have been reused).
+ * grad_rgb [H,W,3] = dL/d rgb is required; grad_depth and grad_alpha
+ * ([H,W] each) may be NULL. Per tile, the transmittance is recomputed by a
+ * forward sweep and the splats are then visited back to front (no per-splat
+ * state is stored by the forward). No counterpart in the reference: it has
+ * no analytic backward (src/optim/gradients.mojo:11-106 stores gradients,
+ * src/optim/trainer.mojo:61-66 injects placeholders). Does not wait. */
+LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* gaussians, const LumenViewCamera* camera,
+                                      const LumenRenderOptions* options, const LumenGpuFrame* frame,
+                                      const float* grad_rgb, const float* grad_depth, const float* grad_alpha,
+                                      LumenGpuGradients* grads, void* stream);
+
+/* Mean L1 loss and its subgradient, compute_l1_loss (src/optim/loss.mojo:11-35):
+ * loss = mean |pred - target|, grad[i] = +1/n if pred[i] - target[i] >= 0
+ * else -1/n. loss is one device float; scratch holds
+ * lumen_gpu_l1_loss_scratch_bytes() bytes (per-block partial sums, summed in
+ * a fixed order so the loss is deterministic). Does not wait. */
+size_t lumen_gpu_l1_loss_scratch_bytes(void);
+LumenStatus lumen_gpu_l1_loss(const float* pred, const float* target, int64_t n, float* grad, float* loss,
+                              void* scratch, void* stream);
+
 /* Stable in-place sort of n (uint64 key, uint32 value) pairs that allocates
  * nothing. No counterpart in the reference. For callers that cannot call
  * cudaMalloc: code inside a host application that owns all device memory

@@ -104,6 +104,10 @@ class LumenGpuCounts(C.Structure):
                 ("depth_sorted_buffer", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class LumenGpuGradients(C.Structure):
+    _fields_ = [("means", _P), ("scales", _P), ("quats", _P), ("opacities", _P), ("sh", _P), ("splat2d", _P)]
+
+
 SPLAT_RECORD_BYTES = 48
 
 # name -> (restype, argtypes); every symbol the two headers declare
@@ -148,6 +152,11 @@ SIGNATURES = {
     "lumen_gpu_sort_pairs": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, C.c_size_t, C.POINTER(C.c_uint32), _P]),
     "lumen_cloud_append": (C.c_int, [_P, C.POINTER(LumenGaussian), C.c_size_t]),
     "lumen_gpu_sort_pairs_noalloc": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "lumen_gpu_render_backward": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenViewCamera),
+                                            C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame), _P, _P, _P,
+                                            C.POINTER(LumenGpuGradients), _P]),
+    "lumen_gpu_l1_loss_scratch_bytes": (C.c_size_t, []),
+    "lumen_gpu_l1_loss": (C.c_int, [_P, _P, C.c_int64, _P, _P, _P, _P]),
     "lumen_gpu_camera_from_lookat": (C.c_int, [C.POINTER(LumenCamera), C.c_uint32, C.c_uint32, C.c_float,
                                                C.c_float, C.POINTER(LumenViewCamera)]),
     "lumen_gpu_stage_timer_create": (_P, [C.c_int]),

@@ -1,0 +1,575 @@
+/*
+ * backward.cu - the adjoint of the forward pipeline (no reference
+ * counterpart: the reference has no analytic backward; its gradient code
+ * only stores buffers, src/optim/gradients.mojo:11-106).
+ *
+ * K6 composite_backward_kernel: per 16x16 tile, per pixel. A forward sweep
+ * recomputes the final transmittance and the last splat each pixel visited
+ * (nothing per splat is stored by the forward); a reverse sweep then walks
+ * the pixel's splats back to front, recovering T_j = T_{j+1} / (1 - alpha_j)
+ * and the suffix colour and depth sums, and forms per splat
+ *   dL/dc = G_rgb w, dL/dz = G_depth w,
+ *   dL/dalpha = sum_ch G_ch (c_ch T_j - S_ch / (1 - alpha))
+ *             + G_depth (z T_j - S_z / (1 - alpha))
+ *             + (G_alpha - [white] sum_ch G_ch) T_final / (1 - alpha),
+ * then through alpha = min(op exp(-power), 0.99) (no gradient when clamped)
+ * and power = 0.5 (a dx^2 + 2 b dx dy + c dy^2) to the centre, the conic and
+ * the opacity. The 10 values per splat are reduced over the warp by
+ * shuffles, over the CTA in shared memory, and added to the splat's
+ * Gaussian with one atomic each per tile.
+ *
+ * K7 project_backward_kernel: per Gaussian, the chain rule through the
+ * conic inverse, the EWA product T Sigma T^T with T = J W, the projective
+ * Jacobian, the screen projection, Sigma = M M^T with M = R(q) S, the
+ * quaternion normalisation, the SH colour (clamped channels get none) and
+ * the view direction, and the exp / sigmoid activations.
+ *
+ * K8 l1_loss_kernel: compute_l1_loss (src/optim/loss.mojo:11-35).
+ */
+#include "composite_common.cuh"
+
+namespace lumen {
+
+constexpr int kGrad2D = 10;   /* cx, cy, ic00, ic01, ic11, opacity, r, g, b, depth */
+
+struct BackwardSmem {
+    float4 geo[kTilePixels];
+    float4 con[kTilePixels];
+    float4 col[kTilePixels];
+    unsigned char mask[kTilePixels];
+    unsigned short list[kTilePixels / 32][kTilePixels];
+    float acc[kTilePixels][kGrad2D];
+    unsigned int gid[kTilePixels];
+    int max_last;
+};
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+/* Stage chunk [cs, cs + 256) of the tile's sorted instances: records, reach
+ * masks, Gaussian ids. Returns the warp's splat list length. */
+__device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatRecord* __restrict__ records,
+                                           const unsigned int* __restrict__ vals,
+                                           const unsigned int* __restrict__ visible_ids, unsigned int n_visible,
+                                           Control* ctrl, int cs, int re, float tile_x0, float tile_y0) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i = cs + tid;
+    unsigned int m = 0;
+    if (i < re) {
+        const unsigned int v = vals[i];
+        if (v >= n_visible) {
+            atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+        } else {
+            const float4* r4 = reinterpret_cast<const float4*>(records + v);
+            const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
+            s.geo[tid] = geo;
+            s.con[tid] = con;
+            s.col[tid] = __ldg(r4 + 2);
+            s.gid[tid] = visible_ids[v];
+            m = reach_mask(geo, con, tile_x0, tile_y0);
+        }
+    }
+    s.mask[tid] = (unsigned char)m;
+#pragma unroll
+    for (int k = 0; k < kGrad2D; ++k) s.acc[tid][k] = 0.0f;
+    __syncthreads();
+    const int n = re - cs < kTilePixels ? re - cs : kTilePixels;
+    int cnt = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int j = base + lane;
+        const bool bit = j < n && ((s.mask[j] >> warp) & 1u);
+        const unsigned int bal = __ballot_sync(0xffffffffu, bit);
+        if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned short)j;
+        cnt += __popc(bal);
+    }
+    __syncwarp();
+    return cnt;
+}
+
+__global__ void __launch_bounds__(kTilePixels, 4)
+composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, Control* ctrl,
+                          int width, int height, int tiles_x, LumenRenderOptions opt,
+                          const float* __restrict__ grad_rgb, const float* __restrict__ grad_depth,
+                          const float* __restrict__ grad_alpha, float* __restrict__ grad2d) {
+    __shared__ BackwardSmem s;
+    const int tile = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    const int px = tx * kTile + warp_block_x(warp) + (lane & 7);
+    const int py = ty * kTile + warp_block_y(warp) + (lane >> 3);
+    const bool inside = px < width && py < height;
+    const long long pix = (long long)py * width + px;
+    const long long cap = f.instance_capacity;
+    const long long K = (long long)ctrl->n_instances < cap ? (long long)ctrl->n_instances : cap;
+    if (K == 0) return;
+    int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
+    if (rs == -1 || rs >= re) return;
+    if (rs < 0 || (long long)re > K) {
+        if (tid == 0) atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+        return;
+    }
+    const unsigned int n_visible = ctrl->n_visible;
+    const unsigned int* __restrict__ vals = ctrl->tile_sort.sorted_buffer ? f.vals[1] : f.vals[0];
+    const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+    const float tile_x0 = (float)(tx * kTile), tile_y0 = (float)(ty * kTile);
+    const float thr = opt.term_threshold;
+    const bool mode_alpha = opt.term_mode == 1;
+
+    /* ---- sweep 1: the forward, for the final T and the last splat visited ---- */
+    float T = 1.0f;
+    int last = re - 1;
+    bool done = !inside;
+    for (int cs = rs; cs < re; cs += kTilePixels) {
+        if (__syncthreads_count(!done) == 0) break;
+        const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, re, tile_x0, tile_y0);
+        for (int t = 0; t < cnt; ++t) {
+            const int j = s.list[warp][t];
+            if (!done) {
+                const float4 gg = s.geo[j], cc = s.con[j];
+                const float dx = pxc - gg.x, dy = pyc - gg.y;
+                float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
+                bool skip = false;
+                if (power < 0.0f) power = 0.0f;
+                else if (power > 4.5f) skip = true;
+                if (!skip) {
+                    float alpha = gg.w * lumen_expf(-power);
+                    if (alpha > (float)0.99) alpha = (float)0.99;
+                    if (!(alpha < min_alpha())) {
+                        T *= (1.0f - alpha);
+                        const float acc = 1.0f - T;
+                        if (mode_alpha ? (acc >= thr) : (T <= thr)) {
+                            done = true;
+                            last = cs + j;
+                        }
+                    }
+                }
+            }
+            if (__all_sync(0xffffffffu, done)) break;
+        }
+        __syncthreads();
+    }
+    if (!inside) last = rs - 1;   /* outside pixels take part in no splat */
+
+    /* ---- sweep 2: back to front ---- */
+    float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, g_a = 0.0f;
+    if (inside) {
+        g_r = grad_rgb[pix * 3 + 0];
+        g_g = grad_rgb[pix * 3 + 1];
+        g_b = grad_rgb[pix * 3 + 2];
+        if (grad_depth && opt.compute_depth) g_d = grad_depth[pix];
+        if (grad_alpha) g_a = grad_alpha[pix];
+    }
+    const float T_final = T;
+    /* terms of dL/dalpha that scale with T_final / (1 - alpha) */
+    const float g_tail = (g_a - (opt.white_background ? (g_r + g_g + g_b) : 0.0f)) * T_final;
+    float S_r = 0.0f, S_g = 0.0f, S_b = 0.0f, S_z = 0.0f;
+    if (tid == 0) s.max_last = rs - 1;
+    __syncthreads();
+    atomicMax(&s.max_last, last);
+    __syncthreads();
+    const int max_last = s.max_last;
+    if (max_last < rs) return;
+    const int top_chunk = rs + ((max_last - rs) / kTilePixels) * kTilePixels;
+    for (int cs = top_chunk; cs >= rs; cs -= kTilePixels) {
+        const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, re, tile_x0, tile_y0);
+        for (int t = cnt - 1; t >= 0; --t) {
+            const int j = s.list[warp][t];
+            const int inst = cs + j;
+            float gcx = 0.0f, gcy = 0.0f, ga = 0.0f, gb = 0.0f, gc = 0.0f, gop = 0.0f;
+            float gr = 0.0f, gg_ = 0.0f, gbl = 0.0f, gz = 0.0f;
+            bool contrib = false;
+            if (inst <= last) {
+                const float4 geo = s.geo[j], cc = s.con[j];
+                const float dx = pxc - geo.x, dy = pyc - geo.y;
+                float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
+                bool skip = false, pclamp = false;
+                if (power < 0.0f) { power = 0.0f; pclamp = true; }
+                else if (power > 4.5f) skip = true;
+                if (!skip) {
+                    const float gexp = lumen_expf(-power);
+                    const float raw = geo.w * gexp;
+                    const bool aclamp = raw > (float)0.99;
+                    const float alpha = aclamp ? (float)0.99 : raw;
+                    if (!(alpha < min_alpha())) {
+                        contrib = true;
+                        const float4 col = s.col[j];
+                        const float one_m = 1.0f - alpha;
+                        const float Tj = T / one_m;
+                        const float w = alpha * Tj;
+                        gr = g_r * w;
+                        gg_ = g_g * w;
+                        gbl = g_b * w;
+                        gz = g_d * w;
+                        const float inv = 1.0f / one_m;
+                        const float dalpha = g_r * (col.x * Tj - S_r * inv) + g_g * (col.y * Tj - S_g * inv) +
+                                             g_b * (col.z * Tj - S_b * inv) + g_d * (geo.z * Tj - S_z * inv) +
+                                             g_tail * inv;
+                        S_r += col.x * w;
+                        S_g += col.y * w;
+                        S_b += col.z * w;
+                        S_z += geo.z * w;
+                        T = Tj;
+                        if (!aclamp) {
+                            gop = dalpha * gexp;
+                            if (!pclamp) {
+                                const float dpower = -dalpha * geo.w * gexp;
+                                ga = 0.5f * dx * dx * dpower;
+                                gb = dx * dy * dpower;
+                                gc = 0.5f * dy * dy * dpower;
+                                /* d dx / d cx = -1 */
+                                gcx = -(cc.x * dx + cc.y * dy) * dpower;
+                                gcy = -(cc.y * dx + cc.z * dy) * dpower;
+                            }
+                        }
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, contrib)) {
+                const float v[kGrad2D] = {gcx, gcy, ga, gb, gc, gop, gr, gg_, gbl, gz};
+#pragma unroll
+                for (int k = 0; k < kGrad2D; ++k) {
+                    const float r = warp_sum(v[k]);
+                    if (lane == 0 && r != 0.0f) atomicAdd(&s.acc[j][k], r);
+                }
+            }
+        }
+        __syncthreads();
+        /* one atomic per value per (splat, tile) */
+        const int i = cs + tid;
+        if (i < re) {
+            float* dst = grad2d + (size_t)s.gid[tid] * kGrad2D;
+#pragma unroll
+            for (int k = 0; k < kGrad2D; ++k) {
+                const float a = s.acc[tid][k];
+                if (a != 0.0f) atomicAdd(dst + k, a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/* ---------------------------------------------------------------- K7 -- */
+
+__device__ __forceinline__ void rot_from_quat(float w, float x, float y, float z, float R[9]) {
+    R[0] = 1.0f - 2.0f * (y * y + z * z); R[1] = 2.0f * (x * y - w * z); R[2] = 2.0f * (x * z + w * y);
+    R[3] = 2.0f * (x * y + w * z); R[4] = 1.0f - 2.0f * (x * x + z * z); R[5] = 2.0f * (y * z - w * x);
+    R[6] = 2.0f * (x * z - w * y); R[7] = 2.0f * (y * z + w * x); R[8] = 1.0f - 2.0f * (x * x + y * y);
+}
+
+/* gradients of the 16 SH basis functions with respect to the (unit)
+ * direction components, for the constants of spherical_harmonics.mojo:17-26 */
+__device__ __forceinline__ void sh_basis_and_grad(float x, float y, float z, float Y[16], float dX[16],
+                                                  float dY[16], float dZ[16]) {
+    const float C0 = (float)0.28209479177387814, C1 = (float)0.4886025119029199;
+    const float C2_0 = (float)1.0925484305920792, C2_1 = (float)0.31539156525252005;
+    const float C2_2 = (float)0.5462742152960396, C3_0 = (float)0.5900435899266435;
+    const float C3_1 = (float)2.890611442640554, C3_2 = (float)0.4570457994644658;
+    const float C3_3 = (float)0.3731763325901154, C3_4 = (float)1.445305721320277;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    Y[0] = C0; dX[0] = 0.0f; dY[0] = 0.0f; dZ[0] = 0.0f;
+    Y[1] = -C1 * y; dX[1] = 0.0f; dY[1] = -C1; dZ[1] = 0.0f;
+    Y[2] = C1 * z; dX[2] = 0.0f; dY[2] = 0.0f; dZ[2] = C1;
+    Y[3] = -C1 * x; dX[3] = -C1; dY[3] = 0.0f; dZ[3] = 0.0f;
+    Y[4] = C2_0 * x * y; dX[4] = C2_0 * y; dY[4] = C2_0 * x; dZ[4] = 0.0f;
+    Y[5] = -C2_0 * y * z; dX[5] = 0.0f; dY[5] = -C2_0 * z; dZ[5] = -C2_0 * y;
+    Y[6] = C2_1 * (2.0f * zz - xx - yy); dX[6] = -2.0f * C2_1 * x; dY[6] = -2.0f * C2_1 * y; dZ[6] = 4.0f * C2_1 * z;
+    Y[7] = -C2_0 * x * z; dX[7] = -C2_0 * z; dY[7] = 0.0f; dZ[7] = -C2_0 * x;
+    Y[8] = C2_2 * (xx - yy); dX[8] = 2.0f * C2_2 * x; dY[8] = -2.0f * C2_2 * y; dZ[8] = 0.0f;
+    Y[9] = -C3_0 * y * (3.0f * xx - yy);
+    dX[9] = -6.0f * C3_0 * x * y; dY[9] = -3.0f * C3_0 * (xx - yy); dZ[9] = 0.0f;
+    Y[10] = C3_1 * x * y * z; dX[10] = C3_1 * y * z; dY[10] = C3_1 * x * z; dZ[10] = C3_1 * x * y;
+    Y[11] = -C3_2 * y * (4.0f * zz - xx - yy);
+    dX[11] = 2.0f * C3_2 * x * y; dY[11] = -C3_2 * (4.0f * zz - xx - 3.0f * yy); dZ[11] = -8.0f * C3_2 * y * z;
+    Y[12] = C3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+    dX[12] = -6.0f * C3_3 * x * z; dY[12] = -6.0f * C3_3 * y * z; dZ[12] = C3_3 * (6.0f * zz - 3.0f * xx - 3.0f * yy);
+    Y[13] = -C3_2 * x * (4.0f * zz - xx - yy);
+    dX[13] = -C3_2 * (4.0f * zz - 3.0f * xx - yy); dY[13] = 2.0f * C3_2 * x * y; dZ[13] = -8.0f * C3_2 * x * z;
+    Y[14] = C3_4 * z * (xx - yy); dX[14] = 2.0f * C3_4 * x * z; dY[14] = -2.0f * C3_4 * y * z; dZ[14] = C3_4 * (xx - yy);
+    Y[15] = -C3_0 * x * (xx - 3.0f * yy);
+    dX[15] = -3.0f * C3_0 * (xx - yy); dY[15] = 6.0f * C3_0 * x * y; dZ[15] = 0.0f;
+}
+
+__global__ void __launch_bounds__(256)
+project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt,
+                        const int* __restrict__ radii, const float* __restrict__ grad2d, LumenGpuGradients out) {
+    __shared__ DevCamera cam_s;
+    if (threadIdx.x == 0) setup_camera(camera, cam_s);
+    __syncthreads();
+    const DevCamera& cam = cam_s;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.count) return;
+    float* gm = out.means + i * 3;
+    float* gs = out.scales + i * 3;
+    float* gq = out.quats + i * 4;
+    float* gsh = out.sh + i * 48;
+    if (radii[i] <= 0) {
+        gm[0] = gm[1] = gm[2] = 0.0f;
+        gs[0] = gs[1] = gs[2] = 0.0f;
+        gq[0] = gq[1] = gq[2] = gq[3] = 0.0f;
+        out.opacities[i] = 0.0f;
+        for (int k = 0; k < 48; ++k) gsh[k] = 0.0f;
+        return;
+    }
+    const float* G = grad2d + i * 10;
+    const float g_cx = G[0], g_cy = G[1], g_a = G[2], g_b = G[3], g_c = G[4], g_op = G[5];
+    const float g_col[3] = {G[6], G[7], G[8]};
+    const float g_z = G[9];
+
+    /* parameters and activations */
+    const float mx = g.means[i * 3], my = g.means[i * 3 + 1], mz = g.means[i * 3 + 2];
+    float s3[3] = {g.scales[i * 3], g.scales[i * 3 + 1], g.scales[i * 3 + 2]};
+    float op = g.opacities[i];
+    if (opt.params_are_logits) {
+        for (int k = 0; k < 3; ++k) s3[k] = lumen_expf(s3[k]);
+        op = 1.0f / (1.0f + lumen_expf(-op));
+    }
+    const float4 q4 = reinterpret_cast<const float4*>(g.quats)[i];
+    const float qn2 = q4.x * q4.x + q4.y * q4.y + q4.z * q4.z + q4.w * q4.w;
+    const float qlen = sqrtf(qn2);
+    const bool qok = qlen > (float)0.000001;
+    const float qw = qok ? q4.x / qlen : 1.0f, qx = qok ? q4.y / qlen : 0.0f;
+    const float qy = qok ? q4.z / qlen : 0.0f, qz = qok ? q4.w / qlen : 0.0f;
+    float R[9];
+    rot_from_quat(qw, qx, qy, qz, R);
+    float sc[3];
+    bool sclamp[3];
+    for (int k = 0; k < 3; ++k) {
+        sclamp[k] = s3[k] < (float)0.00001;
+        sc[k] = sclamp[k] ? (float)0.00001 : s3[k];
+    }
+    float M[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) M[r * 3 + c] = R[r * 3 + c] * sc[c];
+    float S[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) S[r * 3 + c] = M[r * 3] * M[c * 3] + M[r * 3 + 1] * M[c * 3 + 1] + M[r * 3 + 2] * M[c * 3 + 2];
+    /* camera space (the Hamilton-product transform equals W (mu - position)) */
+    const float* W = cam.W;
+    const float vx = mx - cam.px, vy = my - cam.py, vz = mz - cam.pz;
+    const float x = W[0] * vx + W[1] * vy + W[2] * vz;
+    const float y = W[3] * vx + W[4] * vy + W[5] * vz;
+    float z = W[6] * vx + W[7] * vy + W[8] * vz;
+    const bool zclamp = z < (float)0.0001;
+    const float zj = zclamp ? (float)0.0001 : z;
+    const float iz = 1.0f / zj, iz2 = iz * iz, iz3 = iz2 * iz;
+    const float fx = cam.fx, fy = cam.fy;
+    const float j00 = fx * iz, j02 = -fx * x * iz2, j11 = fy * iz, j12 = -fy * y * iz2;
+    float t0[3], t1[3];
+    for (int k = 0; k < 3; ++k) {
+        t0[k] = j00 * W[k] + j02 * W[6 + k];
+        t1[k] = j11 * W[3 + k] + j12 * W[6 + k];
+    }
+    float St0[3], St1[3];
+    for (int r = 0; r < 3; ++r) {
+        St0[r] = S[r * 3] * t0[0] + S[r * 3 + 1] * t0[1] + S[r * 3 + 2] * t0[2];
+        St1[r] = S[r * 3] * t1[0] + S[r * 3 + 1] * t1[1] + S[r * 3 + 2] * t1[2];
+    }
+    const float A = t0[0] * St0[0] + t0[1] * St0[1] + t0[2] * St0[2] + opt.lowpass;
+    const float B = t0[0] * St1[0] + t0[1] * St1[1] + t0[2] * St1[2];
+    const float Cc = t1[0] * St1[0] + t1[1] * St1[1] + t1[2] * St1[2] + opt.lowpass;
+    const float det = A * Cc - B * B;
+
+    /* conic -> Sigma2D (A, B, C) */
+    float gA = 0.0f, gB = 0.0f, gC = 0.0f;
+    if (!(det > (float)-0.0000001 && det < (float)0.0000001)) {
+        const float id2 = 1.0f / (det * det);
+        gA = (-Cc * Cc * g_a + B * Cc * g_b - B * B * g_c) * id2;
+        gB = (2.0f * B * Cc * g_a - (det + 2.0f * B * B) * g_b + 2.0f * A * B * g_c) * id2;
+        gC = (-B * B * g_a + A * B * g_b - A * A * g_c) * id2;
+    }
+    /* Sigma2D = T Sigma T^T (+ low pass) -> rows of T and Sigma */
+    float dt0[3], dt1[3];
+    for (int k = 0; k < 3; ++k) {
+        dt0[k] = 2.0f * gA * St0[k] + gB * St1[k];
+        dt1[k] = gB * St0[k] + 2.0f * gC * St1[k];
+    }
+    float Gs[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) Gs[r * 3 + c] = gA * t0[r] * t0[c] + gB * t0[r] * t1[c] + gC * t1[r] * t1[c];
+    /* T = J W -> Jacobian entries */
+    const float gj00 = dt0[0] * W[0] + dt0[1] * W[1] + dt0[2] * W[2];
+    const float gj02 = dt0[0] * W[6] + dt0[1] * W[7] + dt0[2] * W[8];
+    const float gj11 = dt1[0] * W[3] + dt1[1] * W[4] + dt1[2] * W[5];
+    const float gj12 = dt1[0] * W[6] + dt1[1] * W[7] + dt1[2] * W[8];
+    /* camera-space point: screen centre (camera.mojo:73-79), Jacobian, depth */
+    const float iz_s = 1.0f / z, iz2_s = iz_s * iz_s;
+    float gx = g_cx * fx * iz_s;
+    float gy = g_cy * fy * iz_s;
+    float gzc = -(g_cx * fx * x + g_cy * fy * y) * iz2_s + g_z;
+    gx += gj02 * (-fx * iz2);
+    gy += gj12 * (-fy * iz2);
+    if (!zclamp) gzc += gj00 * (-fx * iz2) + gj02 * (2.0f * fx * x * iz3) + gj11 * (-fy * iz2) + gj12 * (2.0f * fy * y * iz3);
+    float gmu[3];
+    for (int k = 0; k < 3; ++k) gmu[k] = W[k] * gx + W[3 + k] * gy + W[6 + k] * gzc;
+
+    /* colour: clamp(0.5 + sum sh_i Y_i(d)), d = normalize(mu - position) */
+    {
+        const float len = sqrtf(vx * vx + vy * vy + vz * vz);
+        const bool dok = len > (float)0.000001;
+        const float dx_ = dok ? vx / len : 0.0f, dy_ = dok ? vy / len : 0.0f, dz_ = dok ? vz / len : 0.0f;
+        float Y[16], dX[16], dY[16], dZ[16];
+        sh_basis_and_grad(dx_, dy_, dz_, Y, dX, dY, dZ);
+        const int n = opt.sh_degree == 0 ? 1 : opt.sh_degree == 1 ? 4 : opt.sh_degree == 2 ? 9 : 16;
+        const float* sh = g.sh + i * 48;
+        float gd[3] = {0.0f, 0.0f, 0.0f};
+        for (int ch = 0; ch < 3; ++ch) {
+            float v = 0.5f;
+            for (int k = 0; k < n; ++k) v += sh[k * 3 + ch] * Y[k];
+            const float gcol = (v < 0.0f || v > 1.0f) ? 0.0f : g_col[ch];
+            for (int k = 0; k < 16; ++k) {
+                gsh[k * 3 + ch] = k < n ? gcol * Y[k] : 0.0f;
+                if (k < n) {
+                    gd[0] += gcol * sh[k * 3 + ch] * dX[k];
+                    gd[1] += gcol * sh[k * 3 + ch] * dY[k];
+                    gd[2] += gcol * sh[k * 3 + ch] * dZ[k];
+                }
+            }
+        }
+        if (dok) {
+            const float dot = gd[0] * dx_ + gd[1] * dy_ + gd[2] * dz_;
+            gmu[0] += (gd[0] - dx_ * dot) / len;
+            gmu[1] += (gd[1] - dy_ * dot) / len;
+            gmu[2] += (gd[2] - dz_ * dot) / len;
+        }
+    }
+    gm[0] = gmu[0]; gm[1] = gmu[1]; gm[2] = gmu[2];
+
+    /* Sigma = M M^T, M = R diag(s) */
+    float gM[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            float a = 0.0f;
+            for (int k = 0; k < 3; ++k) a += (Gs[r * 3 + k] + Gs[k * 3 + r]) * M[k * 3 + c];
+            gM[r * 3 + c] = a;
+        }
+    float gsc[3];
+    for (int c = 0; c < 3; ++c) {
+        float a = 0.0f;
+        for (int r = 0; r < 3; ++r) a += gM[r * 3 + c] * R[r * 3 + c];
+        gsc[c] = sclamp[c] ? 0.0f : a;
+    }
+    float gR[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) gR[r * 3 + c] = gM[r * 3 + c] * sc[c];
+    /* R(q) for the unit quaternion (w, x, y, z) */
+    float gqw = 2.0f * (-qz * gR[1] + qy * gR[2] + qz * gR[3] - qx * gR[5] - qy * gR[6] + qx * gR[7]);
+    float gqx = 2.0f * (qy * gR[1] + qz * gR[2] + qy * gR[3] - 2.0f * qx * gR[4] - qw * gR[5] + qz * gR[6] +
+                        qw * gR[7] - 2.0f * qx * gR[8]);
+    float gqy = 2.0f * (-2.0f * qy * gR[0] + qx * gR[1] + qw * gR[2] + qx * gR[3] + qz * gR[5] - qw * gR[6] +
+                        qz * gR[7] - 2.0f * qy * gR[8]);
+    float gqz = 2.0f * (-2.0f * qz * gR[0] - qw * gR[1] + qx * gR[2] + qw * gR[3] - 2.0f * qz * gR[4] + qy * gR[5] +
+                        qx * gR[6] + qy * gR[7]);
+    if (qok) {   /* through q / |q| */
+        const float dot = gqw * qw + gqx * qx + gqy * qy + gqz * qz;
+        gq[0] = (gqw - qw * dot) / qlen;
+        gq[1] = (gqx - qx * dot) / qlen;
+        gq[2] = (gqy - qy * dot) / qlen;
+        gq[3] = (gqz - qz * dot) / qlen;
+    } else {
+        gq[0] = gq[1] = gq[2] = gq[3] = 0.0f;
+    }
+    if (opt.params_are_logits) {
+        for (int k = 0; k < 3; ++k) gs[k] = gsc[k] * s3[k];
+        out.opacities[i] = g_op * op * (1.0f - op);
+    } else {
+        for (int k = 0; k < 3; ++k) gs[k] = gsc[k];
+        out.opacities[i] = g_op;
+    }
+}
+
+/* ---------------------------------------------------------------- K8 -- */
+
+constexpr int kL1Blocks = 1024;
+
+__global__ void __launch_bounds__(256)
+l1_loss_kernel(const float* __restrict__ pred, const float* __restrict__ target, long long n,
+               float* __restrict__ grad, float* __restrict__ partial) {
+    __shared__ float ws[8];
+    const float inv_n = 1.0f / (float)n;
+    float sum = 0.0f;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float diff = pred[i] - target[i];
+        /* loss.mojo:27-33: the diff >= 0 branch takes +1/n */
+        if (diff >= 0.0f) { sum += diff; grad[i] = inv_n; }
+        else { sum -= diff; grad[i] = -inv_n; }
+    }
+    sum = warp_sum(sum);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < 8; ++w) t += ws[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+__global__ void l1_finish_kernel(const float* __restrict__ partial, long long n, float* loss) {
+    __shared__ float ws[32];
+    float t = 0.0f;
+    for (int b = threadIdx.x; b < kL1Blocks; b += blockDim.x) t += partial[b];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float a = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += ws[w];
+        *loss = n > 0 ? a * (1.0f / (float)n) : 0.0f;
+    }
+}
+
+}  // namespace lumen
+
+using namespace lumen;
+
+namespace lumen {
+LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt);
+LumenStatus map_cuda(cudaError_t e);
+}
+
+extern "C" {
+
+LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                      const LumenRenderOptions* opt, const LumenGpuFrame* f, const float* grad_rgb,
+                                      const float* grad_depth, const float* grad_alpha, LumenGpuGradients* out,
+                                      void* stream) {
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    if (!f || !f->scratch || !grad_rgb || !out) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (g->count == 0) return LUMEN_SUCCESS;
+    if (!out->means || !out->scales || !out->quats || !out->opacities || !out->sh || !out->splat2d ||
+        !f->records || !f->visible_ids || !f->radii || !f->ranges || !f->vals[0] || !f->vals[1])
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    Control* ctrl = (Control*)f->scratch;
+    cudaError_t e = cudaMemsetAsync(out->splat2d, 0, (size_t)g->count * kGrad2D * sizeof(float), s);
+    if (e != cudaSuccess) return map_cuda(e);
+    const int tiles_x = (cam->width + kTile - 1) / kTile;
+    const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
+    composite_backward_kernel<<<tiles, kTilePixels, 0, s>>>(f->records, *f, ctrl, cam->width, cam->height, tiles_x,
+                                                            *opt, grad_rgb, grad_depth, grad_alpha, out->splat2d);
+    const long long nb = (g->count + 255) / 256;
+    project_backward_kernel<<<(unsigned int)nb, 256, 0, s>>>(*g, *cam, *opt, f->radii, out->splat2d, *out);
+    return map_cuda(cudaGetLastError());
+}
+
+size_t lumen_gpu_l1_loss_scratch_bytes(void) { return (size_t)kL1Blocks * sizeof(float); }
+
+LumenStatus lumen_gpu_l1_loss(const float* pred, const float* target, int64_t n, float* grad, float* loss,
+                              void* scratch, void* stream) {
+    if (n < 0 || !loss || !scratch || (n > 0 && (!pred || !target || !grad))) return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    float* partial = (float*)scratch;
+    if (n > 0) {
+        l1_loss_kernel<<<kL1Blocks, 256, 0, s>>>(pred, target, n, grad, partial);
+    } else {
+        cudaMemsetAsync(partial, 0, lumen_gpu_l1_loss_scratch_bytes(), s);
+    }
+    l1_finish_kernel<<<1, 256, 0, s>>>(partial, n, loss);
+    return map_cuda(cudaGetLastError());
+}
+
+}  // extern "C"
