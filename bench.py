@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--impl", choices=["lumen", "reference"], default="lumen")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fwd-bwd", action="store_true")
     return p.parse_args()
 
 
@@ -214,6 +215,100 @@ def e2e_rasterize(sc, scales, opac, steps, warmup):
     return out
 
 
+def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
+    """Configuration 3: 500k Gaussians at 1920x1080; one step = forward +
+    L1 loss against the render of the perturbed scene + the hand-written
+    backward to (means, log-scales, quats, opacity logits, SH), all through
+    the C ABI on one stream. Also the same step through the torch autograd
+    API (public call path, one host sync per forward)."""
+    import numpy as np
+    import torch
+    from lumen_b200 import _lib as L
+    from lumen_b200 import autograd as A
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    from lumen_b200.types import RenderOptions
+    n = 500_000
+    sc = scenes.box_scene(n, seed=3)
+    tg = scenes.perturbed(sc, seed=33)
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    opt = RenderOptions(term_mode=1, params_are_logits=True)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    params = [t(sc.means), t(sc.log_scales), t(sc.quats), t(sc.opacity_logits), t(sc.sh).reshape(n, 48)]
+    target = R.render(t(tg.means), t(tg.log_scales), t(tg.quats), t(tg.opacity_logits), t(tg.sh).reshape(n, 48),
+                      cam, opt).rgb.contiguous()
+    first = R.render(*params, cam, opt)
+    V, K, T, P = first.n_visible, first.n_instances, cam.n_tiles, WIDTH * HEIGHT
+    passes = bin(first.varying_digits & 0xFFFF).count("1")
+    lib = L.load()
+    g = R.gaussians_struct(*params)
+    ccam, copt = L.view_camera(cam), L.render_options(opt)
+    fs = first.frame.c_struct()
+    img = L.LumenGpuImage()
+    rgb, depth, alpha = (torch.empty((HEIGHT, WIDTH, 3), device=dev), torch.empty((HEIGHT, WIDTH), device=dev),
+                         torch.empty((HEIGHT, WIDTH), device=dev))
+    img.rgb, img.depth, img.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
+    grads = [torch.empty_like(p) for p in params]
+    splat2d = torch.empty((n, 10), device=dev)
+    out = L.LumenGpuGradients()
+    out.means, out.scales, out.quats, out.opacities, out.sh = (x.data_ptr() for x in grads)
+    out.splat2d = splat2d.data_ptr()
+    gimg = torch.empty_like(rgb)
+    loss = torch.empty((), device=dev)
+    l1s = torch.empty(int(lib.lumen_gpu_l1_loss_scratch_bytes()), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def step():
+        L.check(lib.lumen_gpu_render_forward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs), C.byref(img),
+                                             stream), "forward")
+        L.check(lib.lumen_gpu_l1_loss(rgb.data_ptr(), target.data_ptr(), rgb.numel(), gimg.data_ptr(),
+                                      loss.data_ptr(), l1s.data_ptr(), stream), "l1")
+        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs),
+                                              gimg.data_ptr(), None, None, C.byref(out), stream), "backward")
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    counts = L.LumenGpuCounts()
+    L.check(lib.lumen_gpu_read_counts(C.byref(fs), C.byref(counts), stream), "counts")
+    assert counts.error_flags == 0 and counts.n_instances == K
+    # backward alone, for its share
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record()
+    for _ in range(max(steps // 4, 1)):
+        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs),
+                                              gimg.data_ptr(), None, None, C.byref(out), stream), "backward")
+    b1.record()
+    torch.cuda.synchronize(dev)
+    bwd_ms = b0.elapsed_time(b1) / max(steps // 4, 1)
+    # the public API: torch.autograd with the same step
+    leaves = [p.clone().requires_grad_(True) for p in params]
+    ta_steps = max(steps // 4, 3)
+    for i in range(ta_steps + 2):
+        if i == 2:
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+        r, _, _ = A.render(*leaves, cam, opt)
+        A.l1_loss(r, target).backward()
+    torch.cuda.synchronize(dev)
+    api_ms = (time.perf_counter() - t0) * 1e3 / ta_steps
+    b_fwd = 244 * n + 64 * V + (68 + 24 * passes) * K + 8 * T + 16 * P
+    b_bwd = 80 * K + 12 * P + 88 * V + 472 * n
+    total = b_fwd + 24 * P + b_bwd
+    return {"workload": "config 3: 500k Gaussians, 1920x1080, L1 to the perturbed-scene render",
+            "steps_per_s": 1000.0 / ms, "ms_per_step": ms, "backward_ms": bwd_ms,
+            "autograd_api_steps_per_s": 1000.0 / api_ms, "visible": V, "instances": K,
+            "roofline": {"bytes": total, "achieved": total / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": total / (ms * 1e-3) / 1e9 / hbm_peak}}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -332,6 +427,8 @@ def main():
                          "algorithmic_bytes": alg[dname]},
             "frame_roofline": {"bytes": b_fwd, "achieved": frame_gbs, "peak": hbm_peak, "unit": "GB/s",
                                "frac": frame_gbs / hbm_peak}}
+    if not args.no_fwd_bwd:
+        line["fwd_bwd"] = fwd_bwd_leg(dev, min(steps, 100), args.warmup, hbm_peak)
     if not args.no_e2e:
         e2e = e2e_rasterize(sc, scales, opac, steps, args.warmup)
         if pg:   # replicas: the slowest rank's rate times the number of ranks

@@ -49,6 +49,32 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+/* Sum 16 per-lane values over the warp with 16 shuffles instead of 80: at
+ * each butterfly step a lane keeps one half of its values, sends the other
+ * half to its partner and adds what it receives. Afterwards lane l holds the
+ * warp total of value index ((l >> 4) & 1) * 8 + ((l >> 3) & 1) * 4 +
+ * ((l >> 2) & 1) * 2 + ((l >> 1) & 1) (lanes 2m and 2m+1 hold the same). */
+__device__ __forceinline__ float warp_sum16_transposed(float v[16]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int step = 0; step < 4; ++step) {
+        const int o = 16 >> step;          /* partner distance: 16, 8, 4, 2 */
+        const int half = 8 >> step;        /* values kept: 8, 4, 2, 1 */
+        const bool upper = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const float send = upper ? v[i] : v[i + half];
+            const float keep = upper ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+__device__ __forceinline__ int transposed_index(int lane) {
+    return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+
 /* Stage chunk [cs, cs + 256) of the tile's sorted instances: records, reach
  * masks, Gaussian ids. Returns the warp's splat list length. */
 __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatRecord* __restrict__ records,
@@ -228,12 +254,10 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
-                const float v[kGrad2D] = {gcx, gcy, ga, gb, gc, gop, gr, gg_, gbl, gz};
-#pragma unroll
-                for (int k = 0; k < kGrad2D; ++k) {
-                    const float r = warp_sum(v[k]);
-                    if (lane == 0 && r != 0.0f) atomicAdd(&s.acc[j][k], r);
-                }
+                float v[16] = {gcx, gcy, ga, gb, gc, gop, gr, gg_, gbl, gz, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                const float r = warp_sum16_transposed(v);
+                const int k = transposed_index(lane);
+                if ((lane & 1) == 0 && k < kGrad2D && r != 0.0f) atomicAdd(&s.acc[j][k], r);
             }
         }
         __syncthreads();
@@ -310,7 +334,9 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
         gs[0] = gs[1] = gs[2] = 0.0f;
         gq[0] = gq[1] = gq[2] = gq[3] = 0.0f;
         out.opacities[i] = 0.0f;
-        for (int k = 0; k < 48; ++k) gsh[k] = 0.0f;
+        float4* gsh4 = reinterpret_cast<float4*>(gsh);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gsh4[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return;
     }
     const float* G = grad2d + i * 10;
@@ -405,7 +431,7 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
     float gmu[3];
     for (int k = 0; k < 3; ++k) gmu[k] = W[k] * gx + W[3 + k] * gy + W[6 + k] * gzc;
 
-    /* colour: clamp(0.5 + sum sh_i Y_i(d)), d = normalize(mu - position) */
+    /* colour: clamp(0.5 + sum sh_k Y_k(d)), d = normalize(mu - position) */
     {
         const float len = sqrtf(vx * vx + vy * vy + vz * vz);
         const bool dok = len > (float)0.000001;
@@ -413,26 +439,49 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
         float Y[16], dX[16], dY[16], dZ[16];
         sh_basis_and_grad(dx_, dy_, dz_, Y, dX, dY, dZ);
         const int n = opt.sh_degree == 0 ? 1 : opt.sh_degree == 1 ? 4 : opt.sh_degree == 2 ? 9 : 16;
-        const float* sh = g.sh + i * 48;
-        float gd[3] = {0.0f, 0.0f, 0.0f};
+        float shv[48];
+        const float4* sh4 = reinterpret_cast<const float4*>(g.sh + i * 48);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const float4 a = __ldg(sh4 + k);
+            shv[4 * k] = a.x; shv[4 * k + 1] = a.y; shv[4 * k + 2] = a.z; shv[4 * k + 3] = a.w;
+        }
+        float gcol[3];
+#pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
             float v = 0.5f;
-            for (int k = 0; k < n; ++k) v += sh[k * 3 + ch] * Y[k];
-            const float gcol = (v < 0.0f || v > 1.0f) ? 0.0f : g_col[ch];
-            for (int k = 0; k < 16; ++k) {
-                gsh[k * 3 + ch] = k < n ? gcol * Y[k] : 0.0f;
-                if (k < n) {
-                    gd[0] += gcol * sh[k * 3 + ch] * dX[k];
-                    gd[1] += gcol * sh[k * 3 + ch] * dY[k];
-                    gd[2] += gcol * sh[k * 3 + ch] * dZ[k];
-                }
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if (k < n) v += shv[k * 3 + ch] * Y[k];
+            gcol[ch] = (v < 0.0f || v > 1.0f) ? 0.0f : g_col[ch];
+        }
+        float gd0 = 0.0f, gd1 = 0.0f, gd2 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (k < n) {
+                const float a = gcol[0] * shv[k * 3] + gcol[1] * shv[k * 3 + 1] + gcol[2] * shv[k * 3 + 2];
+                gd0 += a * dX[k];
+                gd1 += a * dY[k];
+                gd2 += a * dZ[k];
             }
         }
+        /* dL/dsh[k][ch] = gcol[ch] Y_k, written as 12 float4 */
+        float4* gsh4 = reinterpret_cast<float4*>(gsh);
+#pragma unroll
+        for (int q = 0; q < 12; ++q) {
+            float e[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int m = 4 * q + r, k = m / 3, ch = m % 3;
+                e[r] = k < n ? gcol[ch] * Y[k] : 0.0f;
+            }
+            gsh4[q] = make_float4(e[0], e[1], e[2], e[3]);
+        }
         if (dok) {
-            const float dot = gd[0] * dx_ + gd[1] * dy_ + gd[2] * dz_;
-            gmu[0] += (gd[0] - dx_ * dot) / len;
-            gmu[1] += (gd[1] - dy_ * dot) / len;
-            gmu[2] += (gd[2] - dz_ * dot) / len;
+            const float dot = gd0 * dx_ + gd1 * dy_ + gd2 * dz_;
+            gmu[0] += (gd0 - dx_ * dot) / len;
+            gmu[1] += (gd1 - dy_ * dot) / len;
+            gmu[2] += (gd2 - dz_ * dot) / len;
         }
     }
     gm[0] = gmu[0]; gm[1] = gmu[1]; gm[2] = gmu[2];
