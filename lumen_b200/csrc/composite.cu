@@ -80,7 +80,10 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
                         const float4* r4 = reinterpret_cast<const float4*>(records + v);
                         const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
                         s.geo[tid] = geo;
-                        s.con[tid] = con;
+                        /* 0.5 folded into the conic: scaling by a power of two commutes
+                         * with rounding, so the power below equals the reference's
+                         * 0.5 * (a dx dx + 2 b dx dy + c dy dy) bit for bit */
+                        s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
                         s.col[tid] = __ldg(r4 + 2);
                         m = reach_mask(geo, con, tile_x0, tile_y0);
                     }
@@ -106,12 +109,12 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
                         /* compute_gaussian_pixel_alpha, compositor.mojo:62-89 */
                         const float dx = pxc - gg.x;
                         const float dy = pyc - gg.y;
-                        float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
+                        float power = cc.x * dx * dx + cc.y * dx * dy + cc.z * dy * dy;
                         bool skip = false;
                         if (power < 0.0f) power = 0.0f;
                         else if (power > 4.5f) skip = true;
                         if (!skip) {
-                            float alpha = gg.w * lumen_expf(-power);
+                            float alpha = gg.w * lumen_expf_core(-power);
                             if (alpha > (float)0.99) alpha = (float)0.99;
                             /* PixelAccumulator.blend, compositor.mojo:25-53 */
                             if (!(alpha < min_alpha())) {

@@ -15,17 +15,18 @@ __device__ __forceinline__ int warp_block_y(int w) { return (w >> 1) * 4; }
 /* Minimum of q(x, y) = a x^2 + 2 b x y + c y^2 over [x0,x1] x [y0,y1]
  * (a > 0, c > 0, ac > b^2): 0 if the origin is inside, otherwise the least
  * of the four edge minima (q is convex along each edge). */
-__device__ __forceinline__ float quad_min_rect(float a, float b, float c, float x0, float x1, float y0, float y1) {
+__device__ __forceinline__ float quad_min_rect(float a, float b, float c, float b_over_a, float b_over_c,
+                                               float x0, float x1, float y0, float y1) {
     if (x0 <= 0.0f && x1 >= 0.0f && y0 <= 0.0f && y1 >= 0.0f) return 0.0f;
     float m = INFINITY;
     const float xs[2] = {x0, x1}, ys[2] = {y0, y1};
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const float x = xs[k];
-        const float y = fminf(fmaxf(-b * x / c, y0), y1);
+        const float y = fminf(fmaxf(-b_over_c * x, y0), y1);
         m = fminf(m, a * x * x + 2.0f * b * x * y + c * y * y);
         const float yy = ys[k];
-        const float xx = fminf(fmaxf(-b * yy / a, x0), x1);
+        const float xx = fminf(fmaxf(-b_over_a * yy, x0), x1);
         m = fminf(m, a * xx * xx + 2.0f * b * xx * yy + c * yy * yy);
     }
     return m;
@@ -44,12 +45,13 @@ __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float
     const float pcut = fminf(4.5f, __logf(op / min_alpha()) + 0.01f);
     if (pcut < 0.0f) return 0u;
     const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
+    const float b_over_a = b * __frcp_rn(a), b_over_c = b * __frcp_rn(c);
     unsigned int m = 0;
 #pragma unroll
     for (int w = 0; w < kTilePixels / 32; ++w) {
         const float x0 = tile_x0 + (float)warp_block_x(w) + 0.5f - geo.x;
         const float y0 = tile_y0 + (float)warp_block_y(w) + 0.5f - geo.y;
-        if (quad_min_rect(a, b, c, x0, x0 + 7.0f, y0, y0 + 3.0f) <= qcut) m |= 1u << w;
+        if (quad_min_rect(a, b, c, b_over_a, b_over_c, x0, x0 + 7.0f, y0, y0 + 3.0f) <= qcut) m |= 1u << w;
     }
     return m;
 }

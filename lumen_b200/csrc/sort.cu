@@ -40,40 +40,65 @@ __device__ __forceinline__ long long sort_count(const SortControl* c, long long 
 
 /* Histogram of every varying digit; clears the look-back regions of the
  * passes that will run; optionally fills the tile ranges with -1. */
+/* One key's varying digits into a warp's private histograms. Consecutive
+ * keys often share digits (the instances of one splat), so equal digits
+ * within the warp are combined with match_any before the shared add. */
+template <typename KeyT, int kBytes>
+__device__ __forceinline__ void count_key(unsigned int (*h)[256], KeyT k, bool valid, unsigned int varying,
+                                          int lane) {
+#pragma unroll
+    for (int d = 0; d < kBytes; ++d) {
+        if (!(varying & (1u << d))) continue;
+        const unsigned int b = valid ? (unsigned int)((k >> (8 * d)) & 0xFF) : (0x100u + lane);
+        const unsigned int peers = __match_any_sync(0xffffffffu, b);
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d][b], (unsigned int)__popc(peers));
+    }
+}
+
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
 histogram_kernel(const KeyT* __restrict__ keys, long long capacity, SortControl* sc, unsigned int* lb,
                  long long lb_tiles_cap, int* ranges, long long n_range_ints) {
     constexpr int kBytes = (int)sizeof(KeyT);
-    __shared__ unsigned int h[kBytes][256];
-    const int tid = threadIdx.x, lane = tid & 31;
+    /* a histogram set per warp (per pair of warps for 8-byte keys, to stay
+     * within 32 KB) so warps do not contend on the same shared bins */
+    constexpr int kWarps = kBytes == 8 ? 4 : 8;
+    __shared__ unsigned int h[kWarps][kBytes][256];
+    const int tid = threadIdx.x, lane = tid & 31, warp = (tid >> 5) % kWarps;
     const long long K = sort_count(sc, capacity);
     const unsigned int varying = K > 1 ? varying_digits(sc, kBytes) : 0u;
-    for (int j = tid; j < kBytes * 256; j += 256) (&h[0][0])[j] = 0u;
+    for (int j = tid; j < kWarps * kBytes * 256; j += 256) (&h[0][0][0])[j] = 0u;
     __syncthreads();
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     const long long gtid = (long long)blockIdx.x * blockDim.x + tid;
     if (varying) {
-        /* warps iterate in lockstep so match_any sees full warps */
-        for (long long base = gtid - lane; base < K; base += nthreads) {
-            const long long i = base + lane;
-            const bool valid = i < K;
-            const KeyT k = valid ? keys[i] : (KeyT)0;
+        /* 4 consecutive keys per lane and iteration; warps stay in lockstep */
+        const long long nwarps_total = nthreads / 32;
+        const long long gwarp = gtid / 32;
+        for (long long base = gwarp * 128; base < K; base += nwarps_total * 128) {
+            KeyT kk[4];
+            bool ok[4];
 #pragma unroll
-            for (int d = 0; d < kBytes; ++d) {
-                if (!(varying & (1u << d))) continue;
-                const unsigned int b = valid ? (unsigned int)((k >> (8 * d)) & 0xFF) : (0x100u + lane);
-                const unsigned int peers = __match_any_sync(0xffffffffu, b);
-                if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d][b], (unsigned int)__popc(peers));
+            for (int r = 0; r < 4; ++r) {
+                const long long i = base + r * 32 + lane;
+                ok[r] = i < K;
+                kk[r] = ok[r] ? keys[i] : (KeyT)0;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                count_key<KeyT, kBytes>(h[warp], kk[r], ok[r], varying, lane);
+                __syncwarp();
             }
         }
     }
     __syncthreads();
     if (varying) {
         for (int j = tid; j < kBytes * 256; j += 256) {
-            const int d = j >> 8;
-            const unsigned int c = (&h[0][0])[j];
-            if ((varying & (1u << d)) && c) atomicAdd(&sc->hist[d][j & 255], c);
+            const int d = j >> 8, b = j & 255;
+            unsigned int c = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) c += h[w][d][b];
+            if ((varying & (1u << d)) && c) atomicAdd(&sc->hist[d][b], c);
         }
         const long long tiles = (K + kSortTile - 1) / kSortTile;
         for (int d = 0; d < kBytes; ++d) {
@@ -261,16 +286,33 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
     const unsigned int* __restrict__ keys = sc->sorted_buffer ? k1 : k0;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     unsigned int touched = 0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < K; i += nthreads) {
-        const unsigned int t = keys[i];
-        if ((long long)t >= n_tiles) {   /* self-check: a tile id outside the grid */
-            atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
-            continue;
+    /* each thread takes 4 consecutive keys per iteration (one 16-byte load
+     * when aligned) and compares each with its neighbours */
+    for (long long i0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4; i0 < K; i0 += nthreads * 4) {
+        unsigned int k[4];
+        if (i0 + 3 < K) {
+            const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
+            k[0] = q.x; k[1] = q.y; k[2] = q.z; k[3] = q.w;
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) k[r] = i0 + r < K ? keys[i0 + r] : 0u;
         }
-        const bool first = i == 0 || keys[i - 1] != t;
-        const bool last = i == K - 1 || keys[i + 1] != t;
-        if (first) { ranges[2 * (size_t)t] = (int)i; ++touched; }
-        if (last) ranges[2 * (size_t)t + 1] = (int)(i + 1);
+        const unsigned int prev = i0 > 0 ? keys[i0 - 1] : 0xFFFFFFFFu;
+        const unsigned int next = i0 + 4 < K ? keys[i0 + 4] : 0xFFFFFFFFu;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const long long i = i0 + r;
+            if (i >= K) break;
+            const unsigned int t = k[r];
+            if ((long long)t >= n_tiles) {   /* self-check: a tile id outside the grid */
+                atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+                continue;
+            }
+            const unsigned int before = r == 0 ? prev : k[r - 1];
+            const unsigned int after = (r == 3 || i + 1 >= K) ? (i + 1 >= K ? 0xFFFFFFFFu : next) : k[r + 1];
+            if (i == 0 || before != t) { ranges[2 * (size_t)t] = (int)i; ++touched; }
+            if (i == K - 1 || after != t) ranges[2 * (size_t)t + 1] = (int)(i + 1);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) touched += __shfl_xor_sync(0xffffffffu, touched, o);
