@@ -39,7 +39,7 @@ METRIC = "1080p frames/s and p99 latency, served vs per-call render; fwd+bwd ste
 UNIT = "frames/s"
 N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
-KERNELS_PER_FRAME = 13   # project, 2 x (histogram + 4 digit passes), emit, tile_ranges, composite
+KERNELS_PER_FRAME = 14   # init, project, 2 x (histogram + 4 digit passes), emit, tile_ranges, composite
 
 
 def parse():
@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fwd-bwd", action="store_true")
+    p.add_argument("--no-multiview", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=1000)
     return p.parse_args()
 
 
@@ -309,6 +312,232 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
                          "frac": total / (ms * 1e-3) / 1e9 / hbm_peak}}
 
 
+def multiview_leg(dev, steps, warmup, hbm_peak):
+    """Configuration 2: 300k Gaussians seen from 64 cameras on a Catmull-Rom
+    orbit of radius 10 at 1280x720, all 64 views in one batch
+    (lumen_gpu_render_batch: one pipeline, view-prefixed tile ids in the sort
+    key). Also the same 64 views rendered one call each, for the batching
+    gain. Both device-timed with CUDA events, inputs resident."""
+    import numpy as np
+    import torch
+    from lumen_b200 import _lib as L
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    from lumen_b200.types import RenderOptions
+    n, n_views, W, H = 300_000, 64, 1280, 720
+    sc = scenes.box_scene(n, seed=2)
+    s, op = sc.activated()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    scene = R.Scene(t(sc.means), t(s), t(sc.quats), t(op).reshape(-1), t(sc.sh).reshape(n, 48))
+    cams = scenes.orbit_cameras(n_views, W, H, radius=10.0)
+    opt = RenderOptions(term_mode=1)
+    views = [(scene, c) for c in cams]
+    first = R.render_batch(views, opt)
+    frame, images = first.frame, first.images
+    lib = L.load()
+    arr = R.batch_views(views, images)
+    copt = L.render_options(opt)
+    fs = frame.frame.c_struct()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    timer = lib.lumen_gpu_stage_timer_create(max(steps, 1))
+    for _ in range(warmup):
+        L.check(lib.lumen_gpu_render_batch(arr, n_views, C.byref(copt), C.byref(fs), stream), "batch")
+    torch.cuda.synchronize(dev)
+    for _ in range(steps):
+        L.check(lib.lumen_gpu_render_batch_timed(arr, n_views, C.byref(copt), C.byref(fs), timer, stream), "batch")
+    stage = (C.c_float * 4)()
+    total = C.c_float(0)
+    nfr = C.c_int(0)
+    L.check(lib.lumen_gpu_stage_timer_read(timer, stage, C.byref(total), C.byref(nfr)), "timer")
+    lib.lumen_gpu_stage_timer_destroy(timer)
+    counts = L.LumenGpuCounts()
+    L.check(lib.lumen_gpu_read_counts(C.byref(fs), C.byref(counts), stream), "counts")
+    assert counts.error_flags == 0 and counts.n_instances == first.n_instances
+    ms = total.value / steps
+    # the same views, one render call each (device-resident, no host sync between calls)
+    singles = [R.render(*scene.tensors, c, opt) for c in cams]
+    per = []
+    for c, r in zip(cams, singles):
+        g1, c1 = scene.struct, L.view_camera(c)
+        im = L.LumenGpuImage()
+        im.rgb, im.depth, im.alpha = r.rgb.data_ptr(), r.depth.data_ptr(), r.alpha.data_ptr()
+        per.append((g1, c1, r.frame.c_struct(), im))
+
+    def one_by_one():
+        for g1, c1, f1, im in per:
+            L.check(lib.lumen_gpu_render_forward(C.byref(g1), C.byref(c1), C.byref(copt), C.byref(f1),
+                                                 C.byref(im), stream), "forward")
+    one_by_one()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(steps // 4, 2)
+    e0.record()
+    for _ in range(reps):
+        one_by_one()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms_single = e0.elapsed_time(e1) / reps
+    V, K = first.n_visible, first.n_instances
+    T = sum(c.n_tiles for c in cams)
+    P = n_views * W * H
+    tile_bits = max(T - 1, 1).bit_length()
+    depth_keys = [r.varying_digits >> 8 for r in singles]
+    depth_bytes = bin(int(np.bitwise_or.reduce(np.array(depth_keys))) & 0xFF).count("1")
+    p = (tile_bits + 7) // 8 + depth_bytes
+    b = 236 * n + 8 * n * n_views + 64 * V + (68 + 24 * p) * K + 8 * T + 16 * P
+    return {"workload": "config 2: 300k Gaussians, 64 orbit views at 1280x720, one batch per step",
+            "views_per_s": n_views * 1000.0 / ms, "ms_per_batch": ms,
+            "per_call_views_per_s": n_views * 1000.0 / ms_single, "per_call_ms_for_64": ms_single,
+            "stages_ms": {k: round(v / steps, 4) for k, v in zip(["project", "sort", "tile_ranges", "composite"],
+                                                                 stage)},
+            "visible": V, "instances": K, "tiles": T, "digit_passes": p, "gpu_launches_per_batch": 14,
+            "roofline": {"bytes": b, "achieved": b / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": b / (ms * 1e-3) / 1e9 / hbm_peak}}
+
+
+def _percentile(xs, q):
+    s = sorted(xs)
+    if not s:
+        return None
+    i = min(len(s) - 1, max(0, int(round(q / 100.0 * (len(s) - 1)))))
+    return s[i]
+
+
+def _poisson_stream(server, ids, scene_of, cams, rate, n, pools, seed):
+    """Submit n requests at Poisson arrival times (rate per second) and
+    collect their results; returns (results, wall seconds)."""
+    import random
+    rng = random.Random(seed)
+    handles = []
+    used = {k: [None] * len(v) for k, v in pools.items()}
+    t0 = time.perf_counter()
+    t_next = t0
+    for i in range(n):
+        t_next += rng.expovariate(rate)
+        now = time.perf_counter()
+        if t_next > now:
+            time.sleep(t_next - now)
+        cam = cams[i]
+        key = (cam.width, cam.height)
+        j = i % len(pools[key])
+        prev = used[key][j]
+        if prev is not None and prev[1] is None:   # buffer still owned by an earlier request
+            prev[1] = prev[0].result(timeout_ms=120_000)
+        h = server.submit(ids[scene_of[i]], cam, out=pools[key][j])
+        entry = [h, None]
+        used[key][j] = entry
+        handles.append(entry)
+    res = []
+    for e in handles:
+        if e[1] is None:
+            e[1] = e[0].result(timeout_ms=120_000)
+        res.append(e[1])
+    return res, time.perf_counter() - t0
+
+
+def serving_leg(dev, n_requests, hbm_budget):
+    """Render serving (configuration 4 and a 1080p stream of the 1M scene):
+    Poisson arrivals at 2000 req/s through lumen_serve (continuous batching,
+    graph launches, autotuned chunk and digit-pass tile), 8-bit RGB delivered
+    to page-locked host buffers; the same request list rendered per call
+    (lumen_gpu_render_forward + copy of the 8-bit image to the host + wait,
+    one request at a time) for comparison. Latency = delivery - arrival."""
+    import random
+    import numpy as np
+    import torch
+    from lumen_b200 import _lib as L
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    from lumen_b200 import serve
+    from lumen_b200.types import RenderOptions
+    opt = RenderOptions(term_mode=1)
+    lib = L.load()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    sizes = scenes.SERVING_SCENE_SIZES
+    dscenes = []
+    for i, n in enumerate(sizes):
+        sc = scenes.box_scene(n, seed=100 + i)
+        s, op = sc.activated()
+        dscenes.append(R.Scene(t(sc.means), t(s), t(sc.quats), t(op).reshape(-1), t(sc.sh).reshape(n, 48)))
+    res_list = scenes.SERVING_RESOLUTIONS
+    orbit = {wh: scenes.orbit_cameras(64, wh[0], wh[1], radius=10.0) for wh in res_list}
+    pools = {wh: [torch.empty((wh[1], wh[0], 3), dtype=torch.uint8, pin_memory=True)
+                  for _ in range(48 if wh[1] < 2000 else 24)] for wh in res_list}
+
+    def workload(kind, n, seed):
+        rng = random.Random(seed)
+        sc_of, cams = [], []
+        for _ in range(n):
+            if kind == "mixed":
+                s = rng.randrange(len(sizes))
+                wh = res_list[rng.randrange(len(res_list))]
+            else:
+                s, wh = sizes.index(1_000_000), (1920, 1080)
+            sc_of.append(s)
+            cams.append(orbit[wh][rng.randrange(64)])
+        return sc_of, cams
+
+    per_call_frames = {}
+
+    def per_call(sc_of, cams):
+        """One request at a time: render, copy the 8-bit image to the host, wait."""
+        stream = torch.cuda.current_stream(dev)
+        lat = []
+        t0 = time.perf_counter()
+        for s, cam in zip(sc_of, cams):
+            key = (s, cam.width, cam.height)
+            if key not in per_call_frames:
+                first = R.render(*dscenes[s].tensors, cam, opt)
+                rgb8 = torch.empty((cam.height, cam.width, 3), dtype=torch.uint8, device=dev)
+                per_call_frames[key] = (first.frame, rgb8, pools[(cam.width, cam.height)][0])
+            frame, rgb8, host = per_call_frames[key]
+            c0 = time.perf_counter()
+            img = L.LumenGpuImage()
+            img.rgb8 = rgb8.data_ptr()
+            fs = frame.c_struct()
+            L.check(lib.lumen_gpu_render_forward(C.byref(dscenes[s].struct), C.byref(L.view_camera(cam)),
+                                                 C.byref(L.render_options(opt)), C.byref(fs), C.byref(img),
+                                                 stream.cuda_stream), "forward")
+            host.copy_(rgb8, non_blocking=True)
+            stream.synchronize()
+            lat.append((time.perf_counter() - c0) * 1e3)
+        return lat, time.perf_counter() - t0
+
+    out = {}
+    for kind, rate in (("1080p_1M", 2000.0), ("mixed", 2000.0)):
+        sc_of, cams = workload(kind, n_requests, seed=7 if kind == "mixed" else 8)
+        warm_of, warm_cams = workload(kind, max(n_requests // 2, 64), seed=99)
+        with serve.Server(work_budget_bytes=hbm_budget, max_views_per_batch=64, max_batches_in_flight=2,
+                          use_graphs=True, autotune=True, options=opt) as srv:
+            ids = [srv.add_scene(s) for s in dscenes]
+            _poisson_stream(srv, ids, warm_of, warm_cams, rate, len(warm_cams), pools, seed=5)   # warm-up
+            s0 = srv.stats()
+            res, wall = _poisson_stream(srv, ids, sc_of, cams, rate, n_requests, pools, seed=6)
+            s1 = srv.stats()
+        assert all(r.status == 0 for r in res), "served request failed"
+        lat = [r.latency_ms for r in res]
+        span_s = (max(r.done_ms for r in res) - min(r.submit_ms for r in res)) * 1e-3
+        # per-call: frames prepared by one untimed pass over the distinct (scene, resolution) pairs
+        per_call(sc_of[:min(len(sc_of), 64)], cams[:min(len(cams), 64)])
+        pc_lat, pc_wall = per_call(sc_of, cams)
+        batches = s1["batches"] - s0["batches"]
+        out[kind] = {
+            "requests": n_requests, "offered_req_per_s": rate,
+            "served_frames_per_s": n_requests / span_s, "served_p50_ms": _percentile(lat, 50),
+            "served_p99_ms": _percentile(lat, 99), "mean_batch_views": n_requests / max(batches, 1),
+            "batches": batches, "requeued_batches": s1["requeued_batches"] - s0["requeued_batches"],
+            "graph_launches": s1["graph_launches"] - s0["graph_launches"],
+            "device_busy_frac": (s1["device_ms"] - s0["device_ms"]) * 1e-3 / span_s,
+            "per_call_frames_per_s": n_requests / pc_wall, "per_call_p50_ms": _percentile(pc_lat, 50),
+            "per_call_p99_ms": _percentile(pc_lat, 99),
+            "served_over_per_call": (n_requests / span_s) / (n_requests / pc_wall),
+            "launch_variants_used": sorted({(r.composite_chunk, r.sort_items) for r in res})}
+    out["workload"] = ("config 4: 8 resident scenes {50k..2M} (6.4M Gaussians), Poisson 2000 req/s, random scene, "
+                       "orbit camera and resolution in {640x480, 1280x720, 1920x1080, 3840x2160}; and a 1080p "
+                       "stream of the 1M scene; 8-bit RGB to page-locked host memory")
+    return out
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -427,6 +656,10 @@ def main():
                          "algorithmic_bytes": alg[dname]},
             "frame_roofline": {"bytes": b_fwd, "achieved": frame_gbs, "peak": hbm_peak, "unit": "GB/s",
                                "frac": frame_gbs / hbm_peak}}
+    if not args.no_multiview:
+        line["multiview"] = multiview_leg(dev, min(steps, 20), min(args.warmup, 3), hbm_peak)
+    if not args.no_serving:
+        line["serving"] = serving_leg(dev, args.serve_requests, 24 << 30)
     if not args.no_fwd_bwd:
         line["fwd_bwd"] = fwd_bwd_leg(dev, min(steps, 100), args.warmup, hbm_peak)
     if not args.no_e2e:

@@ -110,16 +110,19 @@ typedef struct {
     size_t scratch_bytes;
 } LumenGpuFrame;
 
-/* Per-pixel outputs in device memory. rgb [H,W,3] is required; the others
- * may be NULL. depth [H,W] alpha-weighted depth; alpha [H,W] = 1 - T;
- * n_contrib [H,W] splats blended (the terminating one included);
- * last_idx [H,W] sorted index of the last instance visited, -1 if none. */
+/* Per-pixel outputs in device memory. rgb [H,W,3] or rgb8 is required;
+ * the others may be NULL. depth [H,W] alpha-weighted depth; alpha [H,W] =
+ * 1 - T; n_contrib [H,W] splats blended (the terminating one included);
+ * last_idx [H,W] sorted index of the last instance visited, -1 if none;
+ * rgb8 [H,W,3] bytes (uint8)(clamp(c, 0, 1) * 255), the conversion of
+ * c_api/src/lumen_c.c:541-543 for a frame that starts cleared. */
 typedef struct {
     float* rgb;
     float* depth;
     float* alpha;
     uint32_t* n_contrib;
     int32_t* last_idx;
+    uint8_t* rgb8;
 } LumenGpuImage;
 
 /* Frame counters read back by lumen_gpu_read_counts. error_flags bits:
@@ -203,6 +206,38 @@ LumenStatus lumen_gpu_render_forward_timed(const LumenGpuGaussians* gaussians, c
                                            LumenGpuImage* image, LumenGpuStageTimer* timer, void* stream);
 LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms[4], float* total_ms,
                                        int* n_frames);
+
+/* ---------------------------------------------------------------- batches
+ * Several views rendered by one pipeline: one projection over all views'
+ * Gaussians, one depth sort, one tile sort whose 32-bit keys are batch-wide
+ * tile ids (the view's first tile id + ty * tiles_x + tx, so the view id is
+ * the key's high part), one range pass and one persistent compositor. A
+ * view's image is identical to rendering it alone: within a (view, tile) the
+ * instances are ordered by (depth key, visible index) either way, and the
+ * visible indices of a view keep its Gaussian order.
+ * No counterpart in the reference, which renders one camera per call
+ * (pipeline.mojo:48-231). */
+typedef struct {
+    LumenGpuGaussians gaussians;    /* views may share a scene or not */
+    LumenViewCamera camera;         /* views may differ in resolution */
+    int32_t reserved;
+    LumenGpuImage image;            /* this view's outputs ([H,W,3] rgb required) */
+} LumenGpuBatchView;
+
+/* Buffer lengths a batch needs: slots = sum over views of count rounded up
+ * to 256 (length of records, visible_ids, radii, rects, depth_keys,
+ * depth_order; radii may be NULL in a batch frame, else radii[slot] with
+ * slot = 256 * (the view's first block) + i), tiles = sum over views of
+ * their tiles (ranges holds 2 * tiles). */
+LumenStatus lumen_gpu_batch_sizes(const LumenGpuBatchView* views, int32_t n_views, int64_t* slots, int64_t* tiles);
+size_t lumen_gpu_batch_scratch_bytes(int64_t slots, int64_t instance_capacity, int32_t n_views);
+/* Enqueue a batch on `stream` (no host sync; the view list is copied before
+ * the call returns). Counts and error flags: lumen_gpu_read_counts. */
+LumenStatus lumen_gpu_render_batch(const LumenGpuBatchView* views, int32_t n_views, const LumenRenderOptions* options,
+                                   LumenGpuFrame* frame, void* stream);
+LumenStatus lumen_gpu_render_batch_timed(const LumenGpuBatchView* views, int32_t n_views,
+                                         const LumenRenderOptions* options, LumenGpuFrame* frame,
+                                         LumenGpuStageTimer* timer, void* stream);
 
 /* The device camera lumen_rasterize uses for a look-at LumenCamera and a
  * width x height frame: fx = fy = H / (2 tan(fov_y / 2)), principal point

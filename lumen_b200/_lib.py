@@ -95,7 +95,12 @@ class LumenGpuFrame(C.Structure):
 
 
 class LumenGpuImage(C.Structure):
-    _fields_ = [("rgb", _P), ("depth", _P), ("alpha", _P), ("n_contrib", _P), ("last_idx", _P)]
+    _fields_ = [("rgb", _P), ("depth", _P), ("alpha", _P), ("n_contrib", _P), ("last_idx", _P), ("rgb8", _P)]
+
+
+class LumenGpuBatchView(C.Structure):
+    _fields_ = [("gaussians", LumenGpuGaussians), ("camera", LumenViewCamera), ("reserved", C.c_int32),
+                ("image", LumenGpuImage)]
 
 
 class LumenGpuCounts(C.Structure):
@@ -106,6 +111,26 @@ class LumenGpuCounts(C.Structure):
 
 class LumenGpuGradients(C.Structure):
     _fields_ = [("means", _P), ("scales", _P), ("quats", _P), ("opacities", _P), ("sh", _P), ("splat2d", _P)]
+
+
+# ---- lumen_serve.h ------------------------------------------------------------
+class LumenServerConfig(C.Structure):
+    _fields_ = [("work_budget_bytes", C.c_int64), ("max_views_per_batch", C.c_int32),
+                ("max_batches_in_flight", C.c_int32), ("use_graphs", C.c_int32), ("autotune", C.c_int32),
+                ("composite_chunk", C.c_int32), ("sort_items", C.c_int32), ("options", LumenRenderOptions)]
+
+
+class LumenServeResult(C.Structure):
+    _fields_ = [("request_id", C.c_uint64), ("status", C.c_int32), ("batch_views", C.c_int32),
+                ("submit_ms", C.c_double), ("start_ms", C.c_double), ("done_ms", C.c_double),
+                ("n_instances", C.c_int64), ("composite_chunk", C.c_int32), ("sort_items", C.c_int32)]
+
+
+class LumenServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("requeued_batches", C.c_uint64), ("rejected", C.c_uint64), ("graph_launches", C.c_uint64),
+                ("device_ms", C.c_double), ("slot_bytes", C.c_int64), ("max_slots", C.c_int64),
+                ("max_tiles", C.c_int64), ("max_instances", C.c_int64), ("max_pixels", C.c_int64)]
 
 
 SPLAT_RECORD_BYTES = 48
@@ -164,6 +189,24 @@ SIGNATURES = {
     "lumen_gpu_render_forward_timed": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenViewCamera),
                                                  C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame),
                                                  C.POINTER(LumenGpuImage), _P, _P]),
+    "lumen_gpu_batch_sizes": (C.c_int, [C.POINTER(LumenGpuBatchView), C.c_int32, C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_int64)]),
+    "lumen_gpu_batch_scratch_bytes": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32]),
+    "lumen_gpu_render_batch": (C.c_int, [C.POINTER(LumenGpuBatchView), C.c_int32, C.POINTER(LumenRenderOptions),
+                                         C.POINTER(LumenGpuFrame), _P]),
+    "lumen_gpu_render_batch_timed": (C.c_int, [C.POINTER(LumenGpuBatchView), C.c_int32,
+                                               C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame), _P, _P]),
+    # lumen_serve.h
+    "lumen_server_default_config": (LumenServerConfig, []),
+    "lumen_server_create": (_P, [C.POINTER(LumenServerConfig)]),
+    "lumen_server_destroy": (None, [_P]),
+    "lumen_server_add_scene": (C.c_int32, [_P, C.POINTER(LumenGpuGaussians)]),
+    "lumen_server_submit": (C.c_int, [_P, C.c_int32, C.POINTER(LumenViewCamera), _P, C.POINTER(C.c_uint64)]),
+    "lumen_server_wait": (C.c_int, [_P, C.c_uint64, C.c_double, C.POINTER(LumenServeResult)]),
+    "lumen_server_stats": (C.c_int, [_P, C.POINTER(LumenServeStats)]),
+    "lumen_serve_admit": (C.c_int32, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64), C.c_int32, C.c_int32, C.c_int64, C.c_int64,
+                                      C.c_int64, C.c_int64]),
     "lumen_gpu_stage_timer_read": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int)]),
 }
 

@@ -5,11 +5,13 @@
  * src/raster/pipeline.mojo:172-229, with compute_gaussian_pixel_alpha and
  * PixelAccumulator.blend/finalize, src/raster/compositor.mojo:10-89.
  *
- * One CTA per 16x16 tile, one thread per pixel, each warp an 8x4 block. The
- * tile's sorted instances are processed in chunks of 256: each thread
- * gathers one instance's 48-byte record (through the sorted visible index)
- * into shared memory and computes which warp blocks the splat can reach at
- * all (reach_mask); each warp then walks, in sorted order, only the splats
+ * One CTA per 16x16 tile (or persistent CTAs taking tiles in ticket order),
+ * one thread per pixel, each warp an 8x4 block. The tile's sorted instances
+ * are processed in chunks of 128, 256 or 512 (a launch parameter the
+ * autotuner picks): the threads gather the chunk's 48-byte records (through
+ * the sorted visible index) into shared memory and compute which warp
+ * blocks each splat can reach at all (reach_mask); each warp then walks, in
+ * sorted order, only the splats
  * that can reach it, so each pixel blends exactly the reference's sequence.
  * A pixel stops after the blend that saturates it; a warp leaves the chunk
  * once all its pixels stopped, and the CTA stops loading chunks once all 256
@@ -23,38 +25,58 @@
 
 namespace lumen {
 
+/* (uint8)(clamp(c, 0, 1) * 255), truncating (c_api/src/lumen_c.c:541-543). */
+__device__ __forceinline__ unsigned char to_byte(float c) {
+    if (c < 0.0f) c = 0.0f;
+    if (c > 1.0f) c = 1.0f;
+    return (unsigned char)(c * 255.0f);
+}
+
+/* A chunk of kChunk sorted instances is staged at a time. */
+template <int kChunk>
 struct CompositeSmem {
-    float4 geo[kTilePixels];            /* cx, cy, depth, opacity */
-    float4 con[kTilePixels];            /* ic00, ic01, ic11, - */
-    float4 col[kTilePixels];            /* r, g, b, - */
-    unsigned char mask[kTilePixels];    /* bit w: the splat can reach warp w's pixels */
-    unsigned short list[kTilePixels / 32][kTilePixels];
+    float4 geo[kChunk];                 /* cx, cy, depth, opacity */
+    float4 con[kChunk];                 /* 0.5 ic00, ic01, 0.5 ic11, - */
+    float4 col[kChunk];                 /* r, g, b, - */
+    unsigned char mask[kChunk];         /* bit w: the splat can reach warp w's pixels */
+    unsigned short list[kTilePixels / 32][kChunk];
+    unsigned int ticket;
 };
 
-__global__ void __launch_bounds__(kTilePixels, 6)
-composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, long long capacity,
-                 Control* __restrict__ ctrl, int width, int height, int tiles_x,
-                 LumenRenderOptions opt, LumenGpuImage img) {
-    __shared__ CompositeSmem s;
-    const int tile = blockIdx.x;
+/* One tile of the batch (batch-wide id gtile, owned by the last view whose
+ * tile_begin <= gtile). */
+template <int kChunk>
+__device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const ViewTable* __restrict__ vt,
+                                               const LumenSplatRecord* __restrict__ records, const LumenGpuFrame& f,
+                                               long long capacity, Control* __restrict__ ctrl,
+                                               const LumenRenderOptions& opt, int n_views, long long gtile) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tx = tile % tiles_x, ty = tile / tiles_x;
-    const int px = tx * kTile + warp_block_x(warp) + (lane & 7);
-    const int py = ty * kTile + warp_block_y(warp) + (lane >> 3);
-    const bool inside = px < width && py < height;
-    const long long pix = (long long)py * width + px;
-    const long long K = (long long)ctrl->n_instances < capacity ? (long long)ctrl->n_instances : capacity;
+    const int view = n_views == 1 ? 0 : find_view_by_tile(vt, n_views, gtile);
+    int tx, ty, px, py;
+    bool inside, any_instance;
+    {
+        const ViewDesc& vd = vt->view[view];
+        const int tiles_x = vd.tiles_x;
+        const int tile = (int)(gtile - vd.tile_begin);
+        tx = tile % tiles_x;
+        ty = tile / tiles_x;
+        px = tx * kTile + warp_block_x(warp) + (lane & 7);
+        py = ty * kTile + warp_block_y(warp) + (lane >> 3);
+        inside = px < vd.cam.width && py < vd.cam.height;
+        any_instance = vd.inst_begin >= 0;
+    }
 
     float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, dep = 0.0f, acc = 0.0f;
     unsigned int count = 0;
     int last = -1;
     bool background = opt.white_background != 0;
 
-    if (K == 0) {
-        /* pipeline.mojo:162-163: no instances, the output stays zero */
+    if (!any_instance) {
+        /* pipeline.mojo:162-163: no instances in the view, the output stays zero */
         background = false;
     } else {
-        int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
+        const long long K = (long long)ctrl->n_instances < capacity ? (long long)ctrl->n_instances : capacity;
+        int rs = f.ranges[2 * gtile], re = f.ranges[2 * gtile + 1];
         const unsigned int n_visible = ctrl->n_visible;
         if (!(rs == -1 || rs >= re) && (rs < 0 || (long long)re > K)) {
             /* self-check: a range outside the sorted instances */
@@ -68,30 +90,35 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
             const float thr = opt.term_threshold;
             const bool mode_alpha = opt.term_mode == 1;
             bool done = !inside;
-            for (int cs = rs; cs < re; cs += kTilePixels) {
+            for (int cs = rs; cs < re; cs += kChunk) {
                 if (__syncthreads_count(!done) == 0) break;
-                const int i = cs + tid;
-                unsigned int m = 0;
-                if (i < re) {
-                    unsigned int v = vals[i];
-                    if (v >= n_visible) {   /* self-check: an index beyond the visible records */
-                        atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
-                    } else {
-                        const float4* r4 = reinterpret_cast<const float4*>(records + v);
-                        const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
-                        s.geo[tid] = geo;
-                        /* 0.5 folded into the conic: scaling by a power of two commutes
-                         * with rounding, so the power below equals the reference's
-                         * 0.5 * (a dx dx + 2 b dx dy + c dy dy) bit for bit */
-                        s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
-                        s.col[tid] = __ldg(r4 + 2);
-                        m = reach_mask(geo, con, tile_x0, tile_y0);
+#pragma unroll
+                for (int r = 0; r < (kChunk + kTilePixels - 1) / kTilePixels; ++r) {
+                    const int slot = r * kTilePixels + tid;
+                    if (kChunk % kTilePixels != 0 && slot >= kChunk) break;
+                    const int i = cs + slot;
+                    unsigned int m = 0;
+                    if (i < re) {
+                        unsigned int v = vals[i];
+                        if (v >= n_visible) {   /* self-check: an index beyond the visible records */
+                            atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+                        } else {
+                            const float4* r4 = reinterpret_cast<const float4*>(records + v);
+                            const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
+                            s.geo[slot] = geo;
+                            /* 0.5 folded into the conic: scaling by a power of two commutes
+                             * with rounding, so the power below equals the reference's
+                             * 0.5 * (a dx dx + 2 b dx dy + c dy dy) bit for bit */
+                            s.con[slot] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
+                            s.col[slot] = __ldg(r4 + 2);
+                            m = reach_mask(geo, con, tile_x0, tile_y0);
+                        }
                     }
+                    s.mask[slot] = (unsigned char)m;
                 }
-                s.mask[tid] = (unsigned char)m;
                 __syncthreads();
                 /* this warp's splats of the chunk, in sorted order */
-                const int n = re - cs < kTilePixels ? re - cs : kTilePixels;
+                const int n = re - cs < kChunk ? re - cs : kChunk;
                 int cnt = 0;
                 for (int base = 0; base < n; base += 32) {
                     const int j = base + lane;
@@ -144,22 +171,80 @@ composite_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, 
     }
     if (!inside) return;
     /* finalize, compositor.mojo:55-59 */
+    const ViewDesc& vd = vt->view[view];
+    const LumenGpuImage& img = vd.img;
+    const long long pix = (long long)py * vd.cam.width + px;
+    /* last visited instance as an offset within the view's instances
+     * (positions are below 2^30) */
+    if (last >= 0) last -= (int)vd.inst_begin;
     if (background) { cr += T; cg += T; cb += T; }
-    img.rgb[pix * 3 + 0] = cr;
-    img.rgb[pix * 3 + 1] = cg;
-    img.rgb[pix * 3 + 2] = cb;
+    if (img.rgb) {
+        img.rgb[pix * 3 + 0] = cr;
+        img.rgb[pix * 3 + 1] = cg;
+        img.rgb[pix * 3 + 2] = cb;
+    }
+    if (img.rgb8) {
+        img.rgb8[pix * 3 + 0] = to_byte(cr);
+        img.rgb8[pix * 3 + 1] = to_byte(cg);
+        img.rgb8[pix * 3 + 2] = to_byte(cb);
+    }
     if (img.depth) img.depth[pix] = opt.compute_depth ? dep : 0.0f;
     if (img.alpha) img.alpha[pix] = acc;
     if (img.n_contrib) img.n_contrib[pix] = count;
     if (img.last_idx) img.last_idx[pix] = last;
 }
 
-void launch_composite(const LumenGpuFrame& f, Control* ctrl, const LumenViewCamera& cam,
-                      const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st) {
-    const int tiles_x = (cam.width + kTile - 1) / kTile;
-    const int tiles_y = (cam.height + kTile - 1) / kTile;
-    composite_kernel<<<tiles_x * tiles_y, kTilePixels, 0, st>>>(
-        f.records, f, (long long)f.instance_capacity, ctrl, cam.width, cam.height, tiles_x, opt, img);
+/* One CTA per tile of the batch. */
+template <int kChunk>
+__global__ void __launch_bounds__(kTilePixels, 6)
+composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplatRecord* __restrict__ records,
+                 LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
+    __shared__ CompositeSmem<kChunk> s;
+    composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, blockIdx.x);
+}
+
+/* Persistent form for a grid fixed in advance (a captured graph replayed
+ * for batches of any size): CTAs take tiles in ticket order. */
+template <int kChunk>
+__global__ void __launch_bounds__(kTilePixels, 6)
+composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRecord* __restrict__ records,
+                            LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
+    __shared__ CompositeSmem<kChunk> s;
+    const long long total = vt->hdr.total_tiles;
+    const int n_views = vt->hdr.n_views;
+    for (;;) {
+        if (threadIdx.x == 0) s.ticket = atomicAdd(&ctrl->composite_ticket, 1u);
+        __syncthreads();
+        const long long t = s.ticket;
+        if (t >= total) break;
+        composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, t);
+        __syncthreads();
+    }
+}
+
+template <int kChunk>
+static void launch_composite_chunk(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
+                                   const LumenRenderOptions& opt, long long n_tiles, bool persistent, int num_sms,
+                                   cudaStream_t st) {
+    if (persistent) {
+        composite_persistent_kernel<kChunk><<<6 * num_sms, kTilePixels, 0, st>>>(
+            vt, f.records, f, (long long)f.instance_capacity, ctrl, opt);
+    } else {
+        composite_kernel<kChunk><<<(unsigned int)n_tiles, kTilePixels, 0, st>>>(
+            vt, n_views, f.records, f, (long long)f.instance_capacity, ctrl, opt);
+    }
+}
+
+/* chunk: instances staged per round, one of kCompositeChunks. */
+void launch_composite(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
+                      const LumenRenderOptions& opt, long long n_tiles, bool persistent, int chunk, int num_sms,
+                      cudaStream_t st) {
+    if (n_tiles <= 0) return;
+    switch (chunk) {
+        case 128: launch_composite_chunk<128>(vt, n_views, f, ctrl, opt, n_tiles, persistent, num_sms, st); break;
+        case 512: launch_composite_chunk<512>(vt, n_views, f, ctrl, opt, n_tiles, persistent, num_sms, st); break;
+        default: launch_composite_chunk<256>(vt, n_views, f, ctrl, opt, n_tiles, persistent, num_sms, st); break;
+    }
 }
 
 }  // namespace lumen

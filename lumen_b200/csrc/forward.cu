@@ -20,26 +20,30 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <vector>
+#include <cstddef>
 
 #include "splat_common.cuh"
 
 namespace lumen {
-void launch_project(const LumenGpuGaussians& g, const LumenViewCamera& cam, const LumenRenderOptions& opt,
-                    const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, cudaStream_t st);
-void launch_emit(const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, int tiles_x,
-                 cudaStream_t st);
+void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& opt, const LumenGpuFrame& f,
+                    Control* ctrl, unsigned long long* lb, long long n_blocks, bool persistent, int num_sms,
+                    cudaStream_t st);
+void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb,
+                 long long n_blocks, bool persistent, int num_sms, cudaStream_t st);
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
-                   SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges, long long n_range_ints,
-                   unsigned int* err, int num_sms, cudaStream_t st);
+                   SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
+                   const long long* n_range_tiles, unsigned int* err, int items, int num_sms, cudaStream_t st);
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
                    long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
                    int num_sms, cudaStream_t st);
-void launch_ranges(const LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st);
+void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st);
 void launch_key_stats64(const unsigned long long* keys, long long n, SortControl* sc, int num_sms, cudaStream_t st);
 void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_mode, unsigned long long* out,
                           int num_sms, cudaStream_t st);
-void launch_composite(const LumenGpuFrame& f, Control* ctrl, const LumenViewCamera& cam,
-                      const LumenRenderOptions& opt, const LumenGpuImage& img, cudaStream_t st);
+void launch_composite(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
+                      const LumenRenderOptions& opt, long long n_tiles, bool persistent, int chunk, int num_sms,
+                      cudaStream_t st);
 void configure_sort_kernels();
 
 int device_sm_count() {
@@ -49,29 +53,53 @@ int device_sm_count() {
     return n;
 }
 
-static void configure_once() {
+void prime_persistent_launches();
+
+/* Kernel attributes and occupancy figures, set once per process before any
+ * launch (and so before any graph capture). */
+void configure_once() {
     static std::once_flag once;
-    std::call_once(once, [] { configure_sort_kernels(); });
+    std::call_once(once, [] {
+        configure_sort_kernels();
+        prime_persistent_launches();
+    });
 }
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt) {
-    if (!g || !cam || !opt) return LUMEN_ERROR_INVALID_ARGUMENT;
+static LumenStatus check_camera(const LumenViewCamera* cam) {
+    if (!cam) return LUMEN_ERROR_INVALID_ARGUMENT;
+    /* tile coordinates must fit the 12-bit fields of a splat's rectangle */
+    if (cam->width <= 0 || cam->height <= 0 || cam->width > kMaxTilesPerAxis * kTile ||
+        cam->height > kMaxTilesPerAxis * kTile)
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    return LUMEN_SUCCESS;
+}
+
+static LumenStatus check_gaussians(const LumenGpuGaussians* g) {
+    if (!g) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (g->count < 0 || g->count >= (1ll << 31)) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (g->count > 0) {
         if (!g->means || !g->scales || !g->quats || !g->opacities || !g->sh) return LUMEN_ERROR_INVALID_ARGUMENT;
         if (!aligned16(g->quats) || !aligned16(g->sh)) return LUMEN_ERROR_INVALID_ARGUMENT;
     }
-    if (cam->width <= 0 || cam->height <= 0 || cam->width > 65535 * kTile || cam->height > 65535 * kTile)
-        return LUMEN_ERROR_INVALID_ARGUMENT;
-    const long long tiles = (long long)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
-    if (tiles >= (1ll << 31)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    return LUMEN_SUCCESS;
+}
+
+static LumenStatus check_options(const LumenRenderOptions* opt) {
+    if (!opt) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (opt->tile_size != kTile) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (opt->sh_degree < 0 || opt->sh_degree > 3) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (opt->key_mode < 0 || opt->key_mode > 1 || opt->term_mode < 0 || opt->term_mode > 1)
         return LUMEN_ERROR_INVALID_ARGUMENT;
     return LUMEN_SUCCESS;
+}
+
+LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt) {
+    LumenStatus st = check_gaussians(g);
+    if (st == LUMEN_SUCCESS) st = check_camera(cam);
+    if (st == LUMEN_SUCCESS) st = check_options(opt);
+    return st;
 }
 
 /* Device-side failures: capacity still exceeded -> out of memory; a bounded
@@ -91,54 +119,173 @@ LumenStatus map_cuda(cudaError_t e) {
     return LUMEN_ERROR_INVALID_ARGUMENT;
 }
 
-static bool frame_ok(const LumenGpuFrame* f, int64_t n) {
+static bool frame_ok(const LumenGpuFrame* f, int64_t n, bool need_radii) {
     if (!f || !f->scratch || !f->ranges || f->instance_capacity <= 0 || f->instance_capacity >= (1ll << 30)) return false;
     if (!f->keys[0] || !f->keys[1] || !f->vals[0] || !f->vals[1]) return false;
-    if (n > 0 && (!f->records || !f->visible_ids || !f->radii || !f->rects || !f->depth_keys[0] ||
+    if (n > 0 && (!f->records || !f->visible_ids || (need_radii && !f->radii) || !f->rects || !f->depth_keys[0] ||
                   !f->depth_keys[1] || !f->depth_order[0] || !f->depth_order[1]))
         return false;
     return true;
+}
+
+/* Zeroes the control block and the two scans' descriptors; with
+ * write_view, first writes a one-view table. Block 0 then derives every
+ * view's device camera (setup_camera) into the table. */
+__global__ void frame_init_kernel(unsigned long long* zero, long long n_words, ViewTable* vt, BatchHeader hdr,
+                                  ViewDesc v0, int write_view) {
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_words; i += nthreads) zero[i] = 0ull;
+    if (blockIdx.x == 0) {
+        if (write_view && threadIdx.x == 0) {
+            vt->hdr = hdr;
+            vt->view[0] = v0;
+        }
+        __syncthreads();
+        const int nv = vt->hdr.n_views;
+        for (int v = threadIdx.x; v < nv; v += blockDim.x) setup_camera(vt->view[v].cam, vt->view[v].dcam);
+    }
+}
+
+/* The frame's kernels after the view table is in place. n_slots and
+ * n_tiles are the batch's (plain launches) or upper bounds (persistent
+ * launches, whose kernels read the batch's sizes from the table); n_views
+ * is the batch's view count, or 0 when only the table knows it. */
+void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRenderOptions& opt,
+                     const LumenGpuFrame& f, long long n_slots, long long n_tiles, int n_views, bool persistent,
+                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s) {
+    Control* ctrl = (Control*)(base + L.control_off);
+    ViewTable* vt = (ViewTable*)(base + L.table_off);
+    unsigned long long* proj_lb = (unsigned long long*)(base + L.proj_lb_off);
+    unsigned long long* emit_lb = (unsigned long long*)(base + L.emit_lb_off);
+    unsigned int* depth_lb = (unsigned int*)(base + L.depth_lb_off);
+    unsigned int* tile_lb = (unsigned int*)(base + L.tile_lb_off);
+    const int sms = device_sm_count();
+    if (n_slots > 0) {
+        launch_project(vt, n_views, opt, f, ctrl, proj_lb, L.proj_blocks, persistent, sms, s);
+        if (ev) cudaEventRecord(ev[1], s);
+        launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
+                      &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,
+                      lc.sort_items, sms, s);
+        launch_emit(vt, f, ctrl, emit_lb, L.proj_blocks, persistent, sms, s);
+    } else if (ev) {
+        cudaEventRecord(ev[1], s);
+    }
+    /* the tile-sort region holds 4 passes of 2048-key tiles */
+    launch_sort32(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort, tile_lb,
+                  2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.sort_items, sms, s);
+    if (ev) cudaEventRecord(ev[2], s);
+    launch_ranges(f, ctrl, vt, sms, s);
+    if (ev) cudaEventRecord(ev[3], s);
+    launch_composite(vt, n_views, f, ctrl, opt, n_tiles, persistent, lc.composite_chunk, sms, s);
+    if (ev) cudaEventRecord(ev[4], s);
+}
+
+void launch_init(const ScratchLayout& L, unsigned char* base, const BatchHeader* hdr, const ViewDesc* v0,
+                        cudaStream_t s) {
+    const long long words = (long long)(L.zeroed_prefix() / sizeof(unsigned long long));
+    long long grid = (words + 255) / 256;
+    if (grid > 256) grid = 256;
+    if (grid < 1) grid = 1;
+    BatchHeader h{};
+    ViewDesc v{};
+    if (hdr) h = *hdr;
+    if (v0) v = *v0;
+    frame_init_kernel<<<(int)grid, 256, 0, s>>>((unsigned long long*)base, words, (ViewTable*)(base + L.table_off),
+                                               h, v, v0 != nullptr);
 }
 
 static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
                                 LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream) {
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
-    if (!img || !img->rgb || !frame_ok(f, g->count)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (!img || (!img->rgb && !img->rgb8) || !frame_ok(f, g->count, true)) return LUMEN_ERROR_INVALID_ARGUMENT;
     const ScratchLayout L = ScratchLayout::make(g->count, f->instance_capacity);
     if (f->scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
     configure_once();
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char* base = (unsigned char*)f->scratch;
-    Control* ctrl = (Control*)(base + L.control_off);
-    unsigned long long* proj_lb = (unsigned long long*)(base + L.proj_lb_off);
-    unsigned long long* emit_lb = (unsigned long long*)(base + L.emit_lb_off);
-    unsigned int* depth_lb = (unsigned int*)(base + L.depth_lb_off);
-    unsigned int* tile_lb = (unsigned int*)(base + L.tile_lb_off);
     const int tiles_x = (cam->width + kTile - 1) / kTile;
     const long long tiles = (long long)tiles_x * ((cam->height + kTile - 1) / kTile);
-    const int sms = device_sm_count();
+    BatchHeader hdr{};
+    hdr.n_views = 1;
+    hdr.total_blocks = L.proj_blocks;
+    hdr.total_tiles = tiles;
+    ViewDesc v{};
+    v.g = *g;
+    v.cam = *cam;
+    v.tiles_x = tiles_x;
+    v.img = *img;
+    v.block_begin = 0;
+    v.tile_begin = 0;
+    v.inst_begin = -1;
     if (ev) cudaEventRecord(ev[0], s);
-    cudaError_t e = cudaMemsetAsync(base, 0, L.zeroed_prefix(), s);
-    if (e != cudaSuccess) return map_cuda(e);
-    if (g->count > 0) {
-        launch_project(*g, *cam, *opt, *f, ctrl, proj_lb, (int)L.proj_blocks, s);
-        if (ev) cudaEventRecord(ev[1], s);
-        launch_sort32(f->depth_keys[0], f->depth_order[0], f->depth_keys[1], f->depth_order[1], g->count,
-                      &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, 0, &ctrl->error_flags, sms, s);
-        launch_emit(*f, ctrl, emit_lb, (int)L.proj_blocks, tiles_x, s);
-    } else if (ev) {
-        cudaEventRecord(ev[1], s);
+    launch_init(L, base, &hdr, &v, s);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, ev, s);
+    return map_cuda(cudaGetLastError());
+}
+
+/* Offsets of a batch's views: blocks (256 Gaussians each) and tiles. */
+static LumenStatus plan_batch(const LumenGpuBatchView* views, int n_views, const LumenRenderOptions* opt,
+                              std::vector<ViewDesc>* out, BatchHeader* hdr) {
+    if (!views || n_views <= 0 || n_views > kMaxViews) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (opt && check_options(opt) != LUMEN_SUCCESS) return LUMEN_ERROR_INVALID_ARGUMENT;
+    long long blocks = 0, tiles = 0;
+    if (out) out->resize((size_t)n_views);
+    for (int v = 0; v < n_views; ++v) {
+        const LumenGpuBatchView& bv = views[v];
+        if (check_gaussians(&bv.gaussians) != LUMEN_SUCCESS || check_camera(&bv.camera) != LUMEN_SUCCESS)
+            return LUMEN_ERROR_INVALID_ARGUMENT;
+        if (out && !bv.image.rgb && !bv.image.rgb8) return LUMEN_ERROR_INVALID_ARGUMENT;
+        const int tiles_x = (bv.camera.width + kTile - 1) / kTile;
+        const long long vt = (long long)tiles_x * ((bv.camera.height + kTile - 1) / kTile);
+        if (out) {
+            ViewDesc& d = (*out)[(size_t)v];
+            std::memset(&d, 0, sizeof(d));
+            d.g = bv.gaussians;
+            d.cam = bv.camera;
+            d.tiles_x = tiles_x;
+            d.img = bv.image;
+            d.block_begin = blocks;
+            d.tile_begin = tiles;
+            d.inst_begin = -1;
+        }
+        blocks += (bv.gaussians.count + kProjThreads - 1) / kProjThreads;
+        tiles += vt;
     }
-    launch_sort32(f->keys[0], f->vals[0], f->keys[1], f->vals[1], f->instance_capacity, &ctrl->tile_sort, tile_lb,
-                  L.sort_tiles, f->ranges, 2 * tiles, &ctrl->error_flags, sms, s);
-    if (ev) cudaEventRecord(ev[2], s);
-    launch_ranges(*f, ctrl, tiles, sms, s);
-    if (ev) cudaEventRecord(ev[3], s);
-    launch_composite(*f, ctrl, *cam, *opt, *img, s);
-    if (ev) cudaEventRecord(ev[4], s);
-    e = cudaGetLastError();
-    return map_cuda(e);
+    /* visible indices and tile ids are 32-bit on the device */
+    if (blocks * kProjThreads >= (1ll << 31) || tiles >= (1ll << 31)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    std::memset(hdr, 0, sizeof(*hdr));
+    hdr->n_views = n_views;
+    hdr->total_blocks = blocks;
+    hdr->total_tiles = tiles;
+    return LUMEN_SUCCESS;
+}
+
+static LumenStatus batch_impl(const LumenGpuBatchView* views, int n_views, const LumenRenderOptions* opt,
+                              LumenGpuFrame* f, cudaEvent_t* ev, void* stream) {
+    if (!opt) return LUMEN_ERROR_INVALID_ARGUMENT;
+    std::vector<ViewDesc> table;
+    BatchHeader hdr;
+    LumenStatus st = plan_batch(views, n_views, opt, &table, &hdr);
+    if (st != LUMEN_SUCCESS) return st;
+    const long long slots = hdr.total_blocks * kProjThreads;
+    if (!frame_ok(f, slots, false)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    const ScratchLayout L = ScratchLayout::make(slots, f->instance_capacity, n_views);
+    if (f->scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
+    configure_once();
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* base = (unsigned char*)f->scratch;
+    /* header and views in one host block; a copy from pageable memory
+     * returns once the bytes are staged, so the block may go out of scope */
+    std::vector<unsigned char> host(view_table_bytes(n_views));
+    std::memcpy(host.data(), &hdr, sizeof(hdr));
+    std::memcpy(host.data() + offsetof(ViewTable, view), table.data(), table.size() * sizeof(ViewDesc));
+    if (ev) cudaEventRecord(ev[0], s);
+    cudaError_t e = cudaMemcpyAsync(base + L.table_off, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return map_cuda(e);
+    launch_init(L, base, nullptr, nullptr, s);
+    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, kDefaultLaunch, ev, s);
+    return map_cuda(cudaGetLastError());
 }
 
 }  // namespace lumen
@@ -219,6 +366,35 @@ LumenStatus lumen_gpu_render_forward_timed(const LumenGpuGaussians* g, const Lum
                                            LumenGpuStageTimer* t, void* stream) {
     if (!t || t->next >= t->max_frames) return LUMEN_ERROR_INVALID_ARGUMENT;
     LumenStatus st = forward_impl(g, cam, opt, f, img, t->ev + (size_t)t->next * 5, stream);
+    if (st == LUMEN_SUCCESS) t->next++;
+    return st;
+}
+
+LumenStatus lumen_gpu_batch_sizes(const LumenGpuBatchView* views, int32_t n_views, int64_t* slots, int64_t* tiles) {
+    if (!slots || !tiles) return LUMEN_ERROR_INVALID_ARGUMENT;
+    BatchHeader hdr;
+    LumenStatus st = plan_batch(views, n_views, nullptr, nullptr, &hdr);
+    if (st != LUMEN_SUCCESS) return st;
+    *slots = hdr.total_blocks * kProjThreads;
+    *tiles = hdr.total_tiles;
+    return LUMEN_SUCCESS;
+}
+
+size_t lumen_gpu_batch_scratch_bytes(int64_t slots, int64_t instance_capacity, int32_t n_views) {
+    if (slots < 0 || instance_capacity < 0 || n_views <= 0 || n_views > kMaxViews) return 0;
+    return ScratchLayout::make(slots, instance_capacity, n_views).total;
+}
+
+LumenStatus lumen_gpu_render_batch(const LumenGpuBatchView* views, int32_t n_views, const LumenRenderOptions* opt,
+                                   LumenGpuFrame* f, void* stream) {
+    return batch_impl(views, n_views, opt, f, nullptr, stream);
+}
+
+LumenStatus lumen_gpu_render_batch_timed(const LumenGpuBatchView* views, int32_t n_views,
+                                         const LumenRenderOptions* opt, LumenGpuFrame* f, LumenGpuStageTimer* t,
+                                         void* stream) {
+    if (!t || t->next >= t->max_frames) return LUMEN_ERROR_INVALID_ARGUMENT;
+    LumenStatus st = batch_impl(views, n_views, opt, f, t->ev + (size_t)t->next * 5, stream);
     if (st == LUMEN_SUCCESS) t->next++;
     return st;
 }

@@ -41,8 +41,9 @@ namespace {
 
 constexpr long long kMaxPairs = LUMEN_GPU_NOALLOC_MAX_PAIRS;
 constexpr long long kTiles = (kMaxPairs + kSortTile - 1) / kSortTile;
-constexpr size_t kControlBytes = (sizeof(Control) + 255) / 256 * 256;
-/* control block, then 8 digit passes x tiles x 256 look-back descriptors */
+constexpr size_t kControlBytes = align_up(sizeof(Control), 256) + align_up(view_table_bytes(1), 256);
+/* control block and a one-view table, then 8 digit passes x tiles x 256
+ * look-back descriptors */
 constexpr size_t kScratchBytes = kControlBytes + (size_t)8 * (size_t)kTiles * 256 * sizeof(unsigned int);
 constexpr size_t kAltKeysBytes = (size_t)kMaxPairs * sizeof(unsigned long long);
 constexpr size_t kAltValsBytes = (size_t)kMaxPairs * sizeof(unsigned int);

@@ -87,86 +87,120 @@ __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int x, uns
 }
 
 struct ProjSmem {
-    DevCamera cam;
+    ViewDesc vd;                 /* the block's view, copied from the table */
     unsigned int blk;
+    int view;
     unsigned int warp_tot[kProjThreads / 32];
     unsigned long long vis_base;
     unsigned long long key_or, key_or_not;
 };
 
+constexpr int kViewWords = (int)(sizeof(ViewDesc) / 4);
+static_assert(sizeof(ViewDesc) % 4 == 0 && kViewWords <= kProjThreads - 32, "view copy layout");
+
+/* Each CTA takes a 256-Gaussian block by ticket (kPersistent: blocks until
+ * the batch's blocks are exhausted, for a grid fixed in advance). Block b
+ * belongs to the last view whose block_begin <= b, and covers that view's
+ * Gaussians (b - block_begin) * 256 onward; visible indices run over the
+ * whole batch in block order. n_views_hint: the batch's view count, or 0
+ * to read it from the table; with one view, the view is copied to shared
+ * memory while the ticket is being taken. */
+template <bool kPersistent>
 __global__ void __launch_bounds__(kProjThreads)
-project_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt, LumenGpuFrame f, Control* ctrl,
-               unsigned long long* lb, int nblocks) {
+project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOptions opt, LumenGpuFrame f,
+               Control* ctrl, unsigned long long* lb) {
     __shared__ ProjSmem s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) {
-        s.blk = atomicAdd(&ctrl->proj_ticket, 1u);
-        setup_camera(camera, s.cam);
-        s.key_or = 0ull;
-        s.key_or_not = 0ull;
+    const int n_views = n_views_hint > 0 ? n_views_hint : vt->hdr.n_views;
+    const long long total_blocks = vt->hdr.total_blocks;
+    if (n_views == 1) {
+        if (tid >= 32 && tid < 32 + kViewWords)
+            reinterpret_cast<unsigned int*>(&s.vd)[tid - 32] = reinterpret_cast<const unsigned int*>(&vt->view[0])[tid - 32];
+        if (tid == 0) s.view = 0;
     }
-    __syncthreads();
-    const int blk = (int)s.blk;
-    const long long i = (long long)blk * kProjThreads + tid;
+    for (;;) {
+        if (tid == 0) {
+            s.blk = atomicAdd(&ctrl->proj_ticket, 1u);
+            s.key_or = 0ull;
+            s.key_or_not = 0ull;
+        }
+        __syncthreads();
+        const int blk = (int)s.blk;
+        if ((long long)blk >= total_blocks) break;
+        if (n_views > 1) {
+            if (warp == 0) {
+                const int v = find_view_by_block(vt, n_views, blk);
+                const unsigned int* src = reinterpret_cast<const unsigned int*>(&vt->view[v]);
+                for (int w = lane; w < kViewWords; w += 32) reinterpret_cast<unsigned int*>(&s.vd)[w] = src[w];
+                if (lane == 0) s.view = v;
+            }
+            __syncthreads();
+        }
+        const long long slot = (long long)blk * kProjThreads + tid;
+        const long long i = (long long)(blk - s.vd.block_begin) * kProjThreads + tid;
 
-    Projected p;
-    p.visible = false;
-    p.radius = 0;
-    if (i < g.count) {
-        const float* m = g.means + i * 3;
-        const float* sc = g.scales + i * 3;
-        const float4 q = __ldg(reinterpret_cast<const float4*>(g.quats) + i);
-        p = project_gaussian(s.cam, __ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(sc), __ldg(sc + 1),
-                             __ldg(sc + 2), Quat{q.x, q.y, q.z, q.w}, __ldg(g.opacities + i),
-                             g.sh + i * 48, opt);
-        f.radii[i] = p.visible ? p.radius : 0;
-    }
-    unsigned int block_vis = 0;
-    const unsigned int vis_local = block_exclusive_scan(p.visible ? 1u : 0u, s.warp_tot, &block_vis);
-    if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_vis);
-    if (warp == 0) {
-        const unsigned long long e = blk > 0 ? lookback64(lb, blk, &ctrl->error_flags) : 0ull;
-        if (lane == 0) {
-            s.vis_base = e;
-            if (blk > 0) st_volatile_u64(lb + blk, kDescIncl64 | (e + block_vis));
+        Projected p;
+        p.visible = false;
+        p.radius = 0;
+        if (i < s.vd.g.count) {
+            const LumenGpuGaussians& g = s.vd.g;
+            const float* m = g.means + i * 3;
+            const float* sc = g.scales + i * 3;
+            const float4 q = __ldg(reinterpret_cast<const float4*>(g.quats) + i);
+            p = project_gaussian(s.vd.dcam, __ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(sc), __ldg(sc + 1),
+                                 __ldg(sc + 2), Quat{q.x, q.y, q.z, q.w}, __ldg(g.opacities + i),
+                                 g.sh + i * 48, opt);
+            if (f.radii) f.radii[slot] = p.visible ? p.radius : 0;
         }
-    }
-    __syncthreads();
-    const unsigned long long vis_base = s.vis_base;
-    unsigned long long kor = 0ull, knot = 0ull;
-    if (p.visible) {
-        const unsigned long long vid = vis_base + vis_local;
-        float4* dst = reinterpret_cast<float4*>(f.records + vid);
-        dst[0] = make_float4(p.cx, p.cy, p.z, p.op);
-        dst[1] = make_float4(p.ic00, p.ic01, p.ic11, 0.0f);
-        dst[2] = make_float4(p.r, p.g, p.b, 0.0f);
-        f.visible_ids[vid] = (unsigned int)i;
-        f.rects[vid] = pack_rect(p.min_tx, p.min_ty, p.max_tx, p.max_ty);
-        const unsigned int dk = depth_key(p.z, opt.key_mode);
-        f.depth_keys[0][vid] = dk;
-        f.depth_order[0][vid] = (unsigned int)vid;
-        kor = dk;
-        knot = ~(unsigned long long)dk & 0xFFFFFFFFull;
-    }
+        unsigned int block_vis = 0;
+        const unsigned int vis_local = block_exclusive_scan(p.visible ? 1u : 0u, s.warp_tot, &block_vis);
+        if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_vis);
+        if (warp == 0) {
+            const unsigned long long e = blk > 0 ? lookback64(lb, blk, &ctrl->error_flags) : 0ull;
+            if (lane == 0) {
+                s.vis_base = e;
+                if (blk > 0) st_volatile_u64(lb + blk, kDescIncl64 | (e + block_vis));
+            }
+        }
+        __syncthreads();
+        const unsigned long long vis_base = s.vis_base;
+        unsigned long long kor = 0ull, knot = 0ull;
+        if (p.visible) {
+            const unsigned long long vid = vis_base + vis_local;
+            float4* dst = reinterpret_cast<float4*>(f.records + vid);
+            dst[0] = make_float4(p.cx, p.cy, p.z, p.op);
+            dst[1] = make_float4(p.ic00, p.ic01, p.ic11, 0.0f);
+            dst[2] = make_float4(p.r, p.g, p.b, 0.0f);
+            f.visible_ids[vid] = (unsigned int)i;
+            f.rects[vid] = pack_rect(p.min_tx, p.min_ty, p.max_tx, p.max_ty, s.view);
+            const unsigned int dk = depth_key(p.z, opt.key_mode);
+            f.depth_keys[0][vid] = dk;
+            f.depth_order[0][vid] = (unsigned int)vid;
+            kor = dk;
+            knot = ~(unsigned long long)dk & 0xFFFFFFFFull;
+        }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        kor |= __shfl_xor_sync(0xffffffffu, kor, o);
-        knot |= __shfl_xor_sync(0xffffffffu, knot, o);
-    }
-    if (lane == 0 && block_vis) {
-        atomicOr(&s.key_or, kor);
-        atomicOr(&s.key_or_not, knot);
-    }
-    __syncthreads();
-    if (tid == 0) {
-        if (block_vis) {
-            atomicOr(&ctrl->depth_sort.key_or, s.key_or);
-            atomicOr(&ctrl->depth_sort.key_or_not, s.key_or_not);
+        for (int o = 16; o > 0; o >>= 1) {
+            kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+            knot |= __shfl_xor_sync(0xffffffffu, knot, o);
         }
-        if (blk == nblocks - 1) {
-            ctrl->n_visible = (unsigned int)(vis_base + block_vis);
-            ctrl->depth_sort.n = vis_base + block_vis;
+        if (lane == 0 && block_vis) {
+            atomicOr(&s.key_or, kor);
+            atomicOr(&s.key_or_not, knot);
         }
+        __syncthreads();
+        if (tid == 0) {
+            if (block_vis) {
+                atomicOr(&ctrl->depth_sort.key_or, s.key_or);
+                atomicOr(&ctrl->depth_sort.key_or_not, s.key_or_not);
+            }
+            if ((long long)blk == total_blocks - 1) {
+                ctrl->n_visible = (unsigned int)(vis_base + block_vis);
+                ctrl->depth_sort.n = vis_base + block_vis;
+            }
+        }
+        if (!kPersistent) break;
+        __syncthreads();
     }
 }
 
@@ -176,104 +210,148 @@ struct EmitSmem {
     unsigned long long inst_base;
     unsigned int incl[kProjThreads];
     unsigned int vis[kProjThreads];
-    unsigned long long rect[kProjThreads];
+    unsigned int rect_lo[kProjThreads];   /* min_tx | min_ty << 16 */
+    unsigned int width[kProjThreads];     /* tiles per rectangle row */
+    unsigned int tile_base[kProjThreads]; /* batch-wide id of the view's tile 0 */
+    unsigned int tiles_x[kProjThreads];
     unsigned long long key_or, key_or_not;
 };
 
+/* Like project_kernel: 256 consecutive splats of the depth order per ticket.
+ * Tile ids are batch-wide (view tile_begin + ty * tiles_x + tx). */
+template <bool kPersistent>
 __global__ void __launch_bounds__(kProjThreads)
-emit_kernel(LumenGpuFrame f, Control* ctrl, unsigned long long* lb, int tiles_x) {
+emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, unsigned long long* lb) {
     __shared__ EmitSmem s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) {
-        s.blk = atomicAdd(&ctrl->emit_ticket, 1u);
-        s.key_or = 0ull;
-        s.key_or_not = 0ull;
-    }
-    __syncthreads();
     const long long V = ctrl->n_visible;
-    const int blk = (int)s.blk;
-    if ((long long)blk * kProjThreads >= V) return;   /* past the visible splats: no look-back waits on it */
-    const long long p = (long long)blk * kProjThreads + tid;
     const unsigned int* order = ctrl->depth_sort.sorted_buffer ? f.depth_order[1] : f.depth_order[0];
-    unsigned int cnt = 0, v = 0;
-    unsigned long long r = 0ull;
-    if (p < V) {
-        v = order[p];
-        r = f.rects[v];
-        const unsigned int w = (unsigned int)((r >> 32) & 0xFFFF) - (unsigned int)(r & 0xFFFF) + 1u;
-        const unsigned int h = (unsigned int)((r >> 48) & 0xFFFF) - (unsigned int)((r >> 16) & 0xFFFF) + 1u;
-        cnt = w * h;
-    }
-    unsigned int block_inst = 0;
-    const unsigned int excl = block_exclusive_scan(cnt, s.warp_tot, &block_inst);
-    if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_inst);
-    s.incl[tid] = excl + cnt;
-    s.vis[tid] = v;
-    s.rect[tid] = r;
-    if (warp == 0) {
-        const unsigned long long e = blk > 0 ? lookback64(lb, blk, &ctrl->error_flags) : 0ull;
-        if (lane == 0) {
-            s.inst_base = e;
-            if (blk > 0) st_volatile_u64(lb + blk, kDescIncl64 | (e + block_inst));
-        }
-    }
-    __syncthreads();
-    const unsigned long long inst_base = s.inst_base;
     const long long cap = f.instance_capacity;
-    unsigned long long kor = 0ull, knot = 0ull;
-    for (unsigned int j = tid; j < block_inst; j += kProjThreads) {
-        int lo = 0, hi = kProjThreads - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (s.incl[mid] > j) hi = mid; else lo = mid + 1;
+    for (;;) {
+        if (tid == 0) {
+            s.blk = atomicAdd(&ctrl->emit_ticket, 1u);
+            s.key_or = 0ull;
+            s.key_or_not = 0ull;
         }
-        const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
-        const unsigned long long rr = s.rect[lo];
-        const unsigned int min_tx = (unsigned int)(rr & 0xFFFF), min_ty = (unsigned int)((rr >> 16) & 0xFFFF);
-        const unsigned int w = (unsigned int)((rr >> 32) & 0xFFFF) - min_tx + 1u;
-        const unsigned int q = j - start;
-        /* rows outer, columns inner (pipeline.mojo:152-153) */
-        const unsigned int tile = (min_ty + q / w) * (unsigned int)tiles_x + min_tx + q % w;
-        const unsigned long long pos = inst_base + j;
-        kor |= tile;
-        knot |= ~(unsigned long long)tile & 0xFFFFFFFFull;
-        if (pos < (unsigned long long)cap) {
-            f.keys[0][pos] = tile;
-            f.vals[0][pos] = s.vis[lo];
+        __syncthreads();
+        const int blk = (int)s.blk;
+        if ((long long)blk * kProjThreads >= V) break;   /* past the visible splats: no look-back waits on it */
+        const long long p = (long long)blk * kProjThreads + tid;
+        unsigned int cnt = 0, v = 0;
+        if (p < V) {
+            v = order[p];
+            const unsigned long long r = f.rects[v];
+            const int mnx = rect_min_tx(r), mny = rect_min_ty(r);
+            const unsigned int w = (unsigned int)(rect_max_tx(r) - mnx + 1);
+            const unsigned int h = (unsigned int)(rect_max_ty(r) - mny + 1);
+            cnt = w * h;
+            const ViewDesc& vd = vt->view[rect_view(r)];
+            s.rect_lo[tid] = (unsigned int)mnx | ((unsigned int)mny << 16);
+            s.width[tid] = w;
+            s.tile_base[tid] = (unsigned int)vd.tile_begin;
+            s.tiles_x[tid] = (unsigned int)vd.tiles_x;
         }
-    }
+        unsigned int block_inst = 0;
+        const unsigned int excl = block_exclusive_scan(cnt, s.warp_tot, &block_inst);
+        if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_inst);
+        s.incl[tid] = excl + cnt;
+        s.vis[tid] = v;
+        if (warp == 0) {
+            const unsigned long long e = blk > 0 ? lookback64(lb, blk, &ctrl->error_flags) : 0ull;
+            if (lane == 0) {
+                s.inst_base = e;
+                if (blk > 0) st_volatile_u64(lb + blk, kDescIncl64 | (e + block_inst));
+            }
+        }
+        __syncthreads();
+        const unsigned long long inst_base = s.inst_base;
+        unsigned long long kor = 0ull, knot = 0ull;
+        for (unsigned int j = tid; j < block_inst; j += kProjThreads) {
+            int lo = 0, hi = kProjThreads - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s.incl[mid] > j) hi = mid; else lo = mid + 1;
+            }
+            const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
+            const unsigned int rl = s.rect_lo[lo];
+            const unsigned int min_tx = rl & 0xFFFFu, min_ty = rl >> 16;
+            const unsigned int w = s.width[lo];
+            const unsigned int q = j - start;
+            /* rows outer, columns inner (pipeline.mojo:152-153) */
+            const unsigned int tile = s.tile_base[lo] + (min_ty + q / w) * s.tiles_x[lo] + min_tx + q % w;
+            const unsigned long long pos = inst_base + j;
+            kor |= tile;
+            knot |= ~(unsigned long long)tile & 0xFFFFFFFFull;
+            if (pos < (unsigned long long)cap) {
+                f.keys[0][pos] = tile;
+                f.vals[0][pos] = s.vis[lo];
+            }
+        }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        kor |= __shfl_xor_sync(0xffffffffu, kor, o);
-        knot |= __shfl_xor_sync(0xffffffffu, knot, o);
-    }
-    if (lane == 0 && block_inst) {
-        atomicOr(&s.key_or, kor);
-        atomicOr(&s.key_or_not, knot);
-    }
-    __syncthreads();
-    if (tid == 0) {
-        if (block_inst) {
-            atomicOr(&ctrl->tile_sort.key_or, s.key_or);
-            atomicOr(&ctrl->tile_sort.key_or_not, s.key_or_not);
+        for (int o = 16; o > 0; o >>= 1) {
+            kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+            knot |= __shfl_xor_sync(0xffffffffu, knot, o);
         }
-        if ((long long)blk == (V - 1) / kProjThreads) {
-            const unsigned long long K = inst_base + block_inst;
-            ctrl->n_instances = K;
-            ctrl->tile_sort.n = K;
-            if (K > (unsigned long long)cap) atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_CAPACITY);
+        if (lane == 0 && block_inst) {
+            atomicOr(&s.key_or, kor);
+            atomicOr(&s.key_or_not, knot);
         }
+        __syncthreads();
+        if (tid == 0) {
+            if (block_inst) {
+                atomicOr(&ctrl->tile_sort.key_or, s.key_or);
+                atomicOr(&ctrl->tile_sort.key_or_not, s.key_or_not);
+            }
+            if ((long long)blk == (V - 1) / kProjThreads) {
+                const unsigned long long K = inst_base + block_inst;
+                ctrl->n_instances = K;
+                ctrl->tile_sort.n = K;
+                if (K > (unsigned long long)cap) atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_CAPACITY);
+            }
+        }
+        if (!kPersistent) break;
+        __syncthreads();
     }
 }
 
-void launch_project(const LumenGpuGaussians& g, const LumenViewCamera& cam, const LumenRenderOptions& opt,
-                    const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, cudaStream_t st) {
-    project_kernel<<<nblocks, kProjThreads, 0, st>>>(g, cam, opt, f, ctrl, lb, nblocks);
+static int resident_ctas(const void* kernel, int threads) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    return per_sm;
 }
 
-void launch_emit(const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb, int nblocks, int tiles_x,
-                 cudaStream_t st) {
-    emit_kernel<<<nblocks, kProjThreads, 0, st>>>(f, ctrl, lb, tiles_x);
+static int g_project_per_sm = 0, g_emit_per_sm = 0;
+
+/* Occupancy of the persistent kernels, queried once (before any capture). */
+void prime_persistent_launches() {
+    g_project_per_sm = resident_ctas((const void*)project_kernel<true>, kProjThreads);
+    g_emit_per_sm = resident_ctas((const void*)emit_kernel<true>, kProjThreads);
+}
+
+/* Plain launches: one CTA per block (n_blocks known on the host).
+ * Persistent launches: every resident CTA, taking tickets. */
+void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& opt, const LumenGpuFrame& f,
+                    Control* ctrl, unsigned long long* lb, long long n_blocks, bool persistent, int num_sms,
+                    cudaStream_t st) {
+    if (n_blocks <= 0) return;
+    if (persistent) {
+        const int per_sm = g_project_per_sm > 0 ? g_project_per_sm : 1;
+        project_kernel<true><<<per_sm * num_sms, kProjThreads, 0, st>>>(vt, n_views, opt, f, ctrl, lb);
+    } else {
+        project_kernel<false><<<(unsigned int)n_blocks, kProjThreads, 0, st>>>(vt, n_views, opt, f, ctrl, lb);
+    }
+}
+
+void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb,
+                 long long n_blocks, bool persistent, int num_sms, cudaStream_t st) {
+    if (n_blocks <= 0) return;
+    if (persistent) {
+        const int per_sm = g_emit_per_sm > 0 ? g_emit_per_sm : 1;
+        emit_kernel<true><<<per_sm * num_sms, kProjThreads, 0, st>>>(vt, f, ctrl, lb);
+    } else {
+        emit_kernel<false><<<(unsigned int)n_blocks, kProjThreads, 0, st>>>(vt, f, ctrl, lb);
+    }
 }
 
 }  // namespace lumen

@@ -58,7 +58,7 @@ __device__ __forceinline__ void count_key(unsigned int (*h)[256], KeyT k, bool v
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
 histogram_kernel(const KeyT* __restrict__ keys, long long capacity, SortControl* sc, unsigned int* lb,
-                 long long lb_tiles_cap, int* ranges, long long n_range_ints) {
+                 long long lb_tiles_cap, int tile_keys, int* ranges, const long long* n_range_tiles) {
     constexpr int kBytes = (int)sizeof(KeyT);
     /* a histogram set per warp (per pair of warps for 8-byte keys, to stay
      * within 32 KB) so warps do not contend on the same shared bins */
@@ -100,25 +100,27 @@ histogram_kernel(const KeyT* __restrict__ keys, long long capacity, SortControl*
             for (int w = 0; w < kWarps; ++w) c += h[w][d][b];
             if ((varying & (1u << d)) && c) atomicAdd(&sc->hist[d][b], c);
         }
-        const long long tiles = (K + kSortTile - 1) / kSortTile;
+        const long long tiles = (K + tile_keys - 1) / tile_keys;
         for (int d = 0; d < kBytes; ++d) {
             if (!(varying & (1u << d))) continue;
             unsigned int* region = lb + (size_t)d * (size_t)lb_tiles_cap * 256;
             for (long long j = gtid; j < tiles * 256; j += nthreads) region[j] = 0u;
         }
     }
-    if (ranges)
+    if (ranges) {
+        const long long n_range_ints = 2 * *n_range_tiles;
         for (long long j = gtid; j < n_range_ints; j += nthreads) ranges[j] = -1;
+    }
     if (blockIdx.x == 0 && tid == 0) {
         sc->varying = varying;
         sc->sorted_buffer = (unsigned int)(__popc(varying) & 1);
     }
 }
 
-template <typename KeyT>
+template <typename KeyT, int kItems>
 struct PassSmem {
-    KeyT keys[kSortTile];
-    unsigned int vals[kSortTile];
+    KeyT keys[kSortThreads * kItems];
+    unsigned int vals[kSortThreads * kItems];
     unsigned int whist[kSortThreads / 32][256];
     unsigned int digit_start[256];
     long long gbase[256];
@@ -150,12 +152,14 @@ __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, i
     return excl;
 }
 
-template <typename KeyT>
-__global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? 3 : 2)
+/* kItems keys per thread: tiles of 256 * kItems keys. */
+template <typename KeyT, int kItems>
+__global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : 3) : 2)
 onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                      unsigned int* lb_all, long long lb_tiles_cap, unsigned int* err, int digit) {
+    constexpr int kTileKeys = kSortThreads * kItems;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    PassSmem<KeyT>& s = *reinterpret_cast<PassSmem<KeyT>*>(smem_raw);
+    PassSmem<KeyT, kItems>& s = *reinterpret_cast<PassSmem<KeyT, kItems>*>(smem_raw);
     const unsigned int varying = sc->varying;
     if (!(varying & (1u << digit))) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -165,7 +169,7 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
     KeyT* __restrict__ kout = src ? k0 : k1;
     unsigned int* __restrict__ vout = src ? v0 : v1;
     const long long K = sort_count(sc, capacity);
-    const long long ntiles = (K + kSortTile - 1) / kSortTile;
+    const long long ntiles = (K + kTileKeys - 1) / kTileKeys;
     const int shift = 8 * digit;
     unsigned int* lb = lb_all + (size_t)digit * (size_t)lb_tiles_cap * 256;
 
@@ -191,25 +195,25 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         __syncthreads();
         const long long tile = s.tile;
         if (tile >= ntiles) break;
-        const long long base = tile * kSortTile;
+        const long long base = tile * kTileKeys;
 
         /* warp w owns keys [base + w*512, +512); item i of lane l is base + w*512 + i*32 + l */
-        KeyT k[kSortItems];
-        unsigned int v[kSortItems];
-        unsigned short rank[kSortItems];
+        KeyT k[kItems];
+        unsigned int v[kItems];
+        unsigned short rank[kItems];
 #pragma unroll
-        for (int it = 0; it < kSortItems; ++it) {
-            const long long idx = base + warp * (kSortItems * 32) + it * 32 + lane;
+        for (int it = 0; it < kItems; ++it) {
+            const long long idx = base + warp * (kItems * 32) + it * 32 + lane;
             const bool valid = idx < K;
             k[it] = valid ? kin[idx] : (KeyT)0;
             v[it] = valid ? vin[idx] : 0u;
         }
-        const long long wbase = base + warp * (kSortItems * 32);
+        const long long wbase = base + warp * (kItems * 32);
         for (int b = lane; b < 256; b += 32) s.whist[warp][b] = 0u;
         __syncwarp();
         /* warp-level stable multisplit */
 #pragma unroll
-        for (int it = 0; it < kSortItems; ++it) {
+        for (int it = 0; it < kItems; ++it) {
             const bool valid = wbase + it * 32 + lane < K;
             const unsigned int d = valid ? (unsigned int)((k[it] >> shift) & 0xFF) : (0x100u + lane);
             const unsigned int peers = __match_any_sync(0xffffffffu, d);
@@ -254,7 +258,7 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         __syncthreads();
         /* reorder through shared memory */
 #pragma unroll
-        for (int it = 0; it < kSortItems; ++it) {
+        for (int it = 0; it < kItems; ++it) {
             if (wbase + it * 32 + lane < K) {
                 const unsigned int d = (unsigned int)((k[it] >> shift) & 0xFF);
                 const unsigned int pos = s.digit_start[d] + s.whist[warp][d] + rank[it];
@@ -263,7 +267,7 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
             }
         }
         __syncthreads();
-        const int nvalid = (int)((K - base) < kSortTile ? (K - base) : kSortTile);
+        const int nvalid = (int)((K - base) < kTileKeys ? (K - base) : kTileKeys);
         for (int j = tid; j < nvalid; j += kSortThreads) {
             const KeyT kk = s.keys[j];
             const unsigned int d = (unsigned int)((kk >> shift) & 0xFF);
@@ -279,9 +283,11 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
  * range starts where its id first appears and ends after it last appears.
  * Empty tiles keep the (-1, -1) the histogram kernel wrote. */
 __global__ void __launch_bounds__(256)
-tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, long long n_tiles,
+tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, ViewTable* vt,
                    int* ranges, Control* ctrl) {
     const SortControl* sc = &ctrl->tile_sort;
+    const long long n_tiles = vt->hdr.total_tiles;
+    const int n_views = vt->hdr.n_views;
     const long long K = sort_count(sc, capacity);
     const unsigned int* __restrict__ keys = sc->sorted_buffer ? k1 : k0;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
@@ -310,7 +316,13 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
             }
             const unsigned int before = r == 0 ? prev : k[r - 1];
             const unsigned int after = (r == 3 || i + 1 >= K) ? (i + 1 >= K ? 0xFFFFFFFFu : next) : k[r + 1];
-            if (i == 0 || before != t) { ranges[2 * (size_t)t] = (int)i; ++touched; }
+            if (i == 0 || before != t) {
+                ranges[2 * (size_t)t] = (int)i;
+                ++touched;
+                /* the first instance of a view (tile ids are view-major) */
+                const int v = find_view_by_tile(vt, n_views, t);
+                if (i == 0 || (long long)before < vt->view[v].tile_begin) vt->view[v].inst_begin = i;
+            }
             if (i == K - 1 || after != t) ranges[2 * (size_t)t + 1] = (int)(i + 1);
         }
     }
@@ -359,34 +371,42 @@ __global__ void sorted_keys64_kernel(const unsigned int* k0, const unsigned int*
     }
 }
 
-template <typename KeyT>
+template <typename KeyT, int kItems>
 void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
-                      unsigned int* lb, long long lb_tiles_cap, int* ranges, long long n_range_ints,
+                      unsigned int* lb, long long lb_tiles_cap, int* ranges, const long long* n_range_tiles,
                       unsigned int* err, int num_sms, cudaStream_t st) {
-    histogram_kernel<KeyT><<<num_sms * 4, 256, 0, st>>>(k0, capacity, sc, lb, lb_tiles_cap, ranges, n_range_ints);
-    const size_t smem = sizeof(PassSmem<KeyT>);
-    const int ctas_per_sm = sizeof(KeyT) == 4 ? 3 : 2;   /* matches __launch_bounds__: all CTAs resident */
+    histogram_kernel<KeyT><<<num_sms * 4, 256, 0, st>>>(k0, capacity, sc, lb, lb_tiles_cap, kSortThreads * kItems,
+                                                        ranges, n_range_tiles);
+    const size_t smem = sizeof(PassSmem<KeyT, kItems>);
+    /* matches __launch_bounds__: all CTAs resident */
+    const int ctas_per_sm = sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : 3) : 2;
     for (int d = 0; d < (int)sizeof(KeyT); ++d)
-        onesweep_pass_kernel<KeyT><<<num_sms * ctas_per_sm, kSortThreads, smem, st>>>(k0, v0, k1, v1, capacity,
-                                                                                       sc, lb, lb_tiles_cap, err, d);
+        onesweep_pass_kernel<KeyT, kItems><<<num_sms * ctas_per_sm, kSortThreads, smem, st>>>(
+            k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d);
 }
 
+/* items: keys per thread of a digit pass, 8 or 16 (tiles of 2048 or 4096
+ * keys); lb_tiles_cap must hold ceil(capacity / (256 * items)) tiles. */
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
-                   SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges, long long n_range_ints,
-                   unsigned int* err, int num_sms, cudaStream_t st) {
-    launch_sort_impl<unsigned int>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_ints, err,
-                                   num_sms, st);
+                   SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
+                   const long long* n_range_tiles, unsigned int* err, int items, int num_sms, cudaStream_t st) {
+    if (items == 8)
+        launch_sort_impl<unsigned int, 8>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles, err,
+                                          num_sms, st);
+    else
+        launch_sort_impl<unsigned int, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles,
+                                           err, num_sms, st);
 }
 
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
                    long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
                    int num_sms, cudaStream_t st) {
-    launch_sort_impl<unsigned long long>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, 0, err, num_sms,
-                                         st);
+    launch_sort_impl<unsigned long long, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
+                                             num_sms, st);
 }
 
-void launch_ranges(const LumenGpuFrame& f, Control* ctrl, long long n_tiles, int num_sms, cudaStream_t st) {
-    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f.keys[0], f.keys[1], (long long)f.instance_capacity, n_tiles,
+void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st) {
+    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f.keys[0], f.keys[1], (long long)f.instance_capacity, vt,
                                                     f.ranges, ctrl);
 }
 
@@ -401,10 +421,12 @@ void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_m
 }
 
 void configure_sort_kernels() {
-    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(PassSmem<unsigned int>));
-    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(PassSmem<unsigned long long>));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned int, 8>));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned int, 16>));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned long long, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned long long, 16>));
 }
 
 }  // namespace lumen

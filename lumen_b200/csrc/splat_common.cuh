@@ -47,7 +47,8 @@ struct Control {
     unsigned int emit_ticket;            /* block order of the emit look-back */
     unsigned int error_flags;            /* LUMEN_GPU_ERR_* */
     unsigned int touched_tiles;
-    unsigned int pad[9];
+    unsigned int composite_ticket;       /* tile order of the compositor */
+    unsigned int pad[8];
     SortControl depth_sort;              /* visible splats by depth key */
     SortControl tile_sort;               /* instances by tile id */
 };
@@ -56,37 +57,128 @@ constexpr int kProjThreads = 256;
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;   /* 4096 keys per tile */
+constexpr int kSortTileMin = kSortThreads * 8;         /* the smallest tile a digit pass may use */
 
-__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+/* Launch parameters an autotuner may choose; none of them changes a result. */
+struct LaunchConfig {
+    int composite_chunk;   /* instances staged per compositing round: 128, 256 or 512 */
+    int sort_items;        /* keys per thread in a digit pass: 8 or 16 */
+};
+constexpr LaunchConfig kDefaultLaunch = {256, 16};
+
+__host__ __device__ constexpr inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Quat { float w, x, y, z; };
+
+/* Per-view constants, computed on the device in the same order as
+ * PinholeCamera (src/scene/camera.mojo:24-79). */
+struct DevCamera {
+    float px, py, pz;
+    Quat qi;      /* rotation.inverse()            (world_to_cam)       */
+    Quat qii;     /* rotation.inverse().inverse()  (inside rotate_vec)  */
+    float W[9];   /* rotation.inverse().to_rotation_matrix()            */
+    float fx, fy, cx, cy, near_plane, far_plane;
+    int width, height, tiles_x, tiles_y;
+};
+
+/* One view of a batch as the kernels read it. A batch is a list of views,
+ * each with its own scene, camera and output image; a single-view frame is a
+ * batch of one. Projection treats the batch as consecutive 256-Gaussian
+ * blocks (block_begin: the view's first block; its Gaussian i has slot
+ * block_begin * 256 + i), and tiles get batch-wide ids (tile_begin: the
+ * global id of the view's tile 0), so one sort orders every view at once:
+ * the tile-id key carries the view in its high part. */
+struct ViewDesc {
+    LumenGpuGaussians g;
+    LumenViewCamera cam;
+    int tiles_x;
+    LumenGpuImage img;
+    long long block_begin;
+    long long tile_begin;
+    long long inst_begin;     /* first tile-sorted instance of the view, or -1
+                                 (written on the device by the range pass) */
+    DevCamera dcam;           /* derived from cam on the device before projection */
+};
+
+struct BatchHeader {
+    int n_views;
+    int reserved0;
+    long long total_blocks;   /* projection blocks of all views */
+    long long total_tiles;    /* tiles of all views */
+    long long reserved1;
+};
+
+/* Header and views, in scratch; written before the frame's kernels run. */
+struct ViewTable {
+    BatchHeader hdr;
+    ViewDesc view[1];
+};
+
+__host__ __device__ constexpr inline size_t view_table_bytes(int max_views) {
+    return sizeof(BatchHeader) + (size_t)(max_views > 0 ? max_views : 1) * sizeof(ViewDesc);
+}
 
 /* Scratch layout: [Control][project look-back: u64 per block][emit
- * look-back: u64 per block][depth-sort look-back: 4 passes x tiles x 256 x
- * u32][tile-sort look-back: 8 passes x tiles x 256 x u32 (8 so that the
- * standalone 64-bit pair sort can use it)]. */
+ * look-back: u64 per block][view table][depth-sort look-back: 4 passes x
+ * 2048-key tiles x 256 x u32][tile-sort look-back: 8 passes x 4096-key tiles
+ * x 256 x u32, which is also 4 passes x 2048-key tiles (8 passes for the
+ * standalone 64-bit pair sort)]. n counts projection slots (the Gaussians
+ * of all views, each view rounded up to 256). */
 struct ScratchLayout {
-    size_t control_off, proj_lb_off, emit_lb_off, depth_lb_off, tile_lb_off, total;
+    size_t control_off, proj_lb_off, emit_lb_off, table_off, depth_lb_off, tile_lb_off, total;
     int64_t proj_blocks, depth_tiles, sort_tiles;
-    __host__ __device__ static ScratchLayout make(int64_t n, int64_t capacity) {
+    __host__ __device__ static ScratchLayout make(int64_t n, int64_t capacity, int max_views = 1) {
         ScratchLayout L;
         L.proj_blocks = (n + kProjThreads - 1) / kProjThreads;
-        L.depth_tiles = (n + kSortTile - 1) / kSortTile;
+        L.depth_tiles = (n + kSortTileMin - 1) / kSortTileMin;
         L.sort_tiles = (capacity + kSortTile - 1) / kSortTile;
         L.control_off = 0;
         L.proj_lb_off = align_up(sizeof(Control), 256);
         L.emit_lb_off = align_up(L.proj_lb_off + (size_t)L.proj_blocks * sizeof(unsigned long long), 256);
-        L.depth_lb_off = align_up(L.emit_lb_off + (size_t)L.proj_blocks * sizeof(unsigned long long), 256);
+        L.table_off = align_up(L.emit_lb_off + (size_t)L.proj_blocks * sizeof(unsigned long long), 256);
+        L.depth_lb_off = align_up(L.table_off + view_table_bytes(max_views), 256);
         L.tile_lb_off = align_up(L.depth_lb_off + (size_t)4 * (size_t)L.depth_tiles * 256 * sizeof(unsigned int), 256);
         L.total = align_up(L.tile_lb_off + (size_t)8 * (size_t)L.sort_tiles * 256 * sizeof(unsigned int), 256);
         return L;
     }
-    /* bytes the host must zero before a frame (control and both scans) */
-    size_t zeroed_prefix() const { return depth_lb_off; }
+    /* bytes zeroed before a frame: control and both scans */
+    size_t zeroed_prefix() const { return table_off; }
 };
 
-/* Tile rectangle of a visible splat, 16 bits per bound. */
-__host__ __device__ inline unsigned long long pack_rect(int min_tx, int min_ty, int max_tx, int max_ty) {
-    return (unsigned long long)(unsigned short)min_tx | ((unsigned long long)(unsigned short)min_ty << 16) |
-           ((unsigned long long)(unsigned short)max_tx << 32) | ((unsigned long long)(unsigned short)max_ty << 48);
+/* Tile rectangle of a visible splat and its view: 12 bits per bound (tile
+ * coordinates below 4096, images up to 65520 pixels a side), view in the
+ * top 16 bits. */
+constexpr int kMaxTilesPerAxis = 4095;
+constexpr int kMaxViews = 65535;
+
+__host__ __device__ inline unsigned long long pack_rect(int min_tx, int min_ty, int max_tx, int max_ty, int view) {
+    return (unsigned long long)(min_tx & 0xFFF) | ((unsigned long long)(min_ty & 0xFFF) << 12) |
+           ((unsigned long long)(max_tx & 0xFFF) << 24) | ((unsigned long long)(max_ty & 0xFFF) << 36) |
+           ((unsigned long long)(view & 0xFFFF) << 48);
+}
+__host__ __device__ inline int rect_min_tx(unsigned long long r) { return (int)(r & 0xFFF); }
+__host__ __device__ inline int rect_min_ty(unsigned long long r) { return (int)((r >> 12) & 0xFFF); }
+__host__ __device__ inline int rect_max_tx(unsigned long long r) { return (int)((r >> 24) & 0xFFF); }
+__host__ __device__ inline int rect_max_ty(unsigned long long r) { return (int)((r >> 36) & 0xFFF); }
+__host__ __device__ inline int rect_view(unsigned long long r) { return (int)(r >> 48); }
+
+/* The view whose [begin, next begin) holds x: the last view with begin <= x
+ * (views with no blocks or tiles are skipped over). */
+__device__ __forceinline__ int find_view_by_block(const ViewTable* vt, int n_views, long long blk) {
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (vt->view[mid].block_begin <= blk) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int find_view_by_tile(const ViewTable* vt, int n_views, long long tile) {
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (vt->view[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
 }
 
 /* Bounded spin: after this many polls a wait gives up, sets
@@ -103,7 +195,6 @@ constexpr unsigned int kDescMask32 = (1u << 30) - 1;
 
 /* ---------------------------------------------------------------- math -- */
 
-struct Quat { float w, x, y, z; };
 
 /* Quatf.normalized, src/math/quaternion.mojo:46-57 */
 __device__ __forceinline__ Quat q_normalized(Quat q) {
@@ -145,17 +236,6 @@ __device__ __forceinline__ void q_to_matrix(Quat q0, float m[9]) {
     m[3] = xy + wz;          m[4] = 1.0f - (xx + zz); m[5] = yz - wx;
     m[6] = xz - wy;          m[7] = yz + wx;          m[8] = 1.0f - (xx + yy);
 }
-
-/* Per-view constants, computed on the device in the same order as
- * PinholeCamera (src/scene/camera.mojo:24-79). */
-struct DevCamera {
-    float px, py, pz;
-    Quat qi;      /* rotation.inverse()            (world_to_cam)       */
-    Quat qii;     /* rotation.inverse().inverse()  (inside rotate_vec)  */
-    float W[9];   /* rotation.inverse().to_rotation_matrix()            */
-    float fx, fy, cx, cy, near_plane, far_plane;
-    int width, height, tiles_x, tiles_y;
-};
 
 __device__ __forceinline__ void setup_camera(const LumenViewCamera& c, DevCamera& d) {
     Quat r = q_normalized({c.rotation[0], c.rotation[1], c.rotation[2], c.rotation[3]});  /* camera.mojo:229 */

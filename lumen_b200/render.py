@@ -184,6 +184,160 @@ def render(means: torch.Tensor, scales: torch.Tensor, quats: torch.Tensor, opaci
                         options)
 
 
+class Scene:
+    """A scene resident on the device: SoA parameter tensors (float32,
+    contiguous) in the layout of LumenGpuGaussians."""
+
+    def __init__(self, means, scales, quats, opacities, sh):
+        n = int(means.shape[0])
+        self.tensors = (means, scales, quats, opacities, sh.reshape(n, 48) if n else sh.reshape(0, 48))
+        self.struct = gaussians_struct(*self.tensors)
+        self.count = n
+
+    @property
+    def device(self):
+        return self.tensors[0].device
+
+
+@dataclass
+class BatchFrame:
+    """Work buffers of a batch (LumenGpuFrame sized by lumen_gpu_batch_sizes)."""
+    frame: Frame
+    slots: int
+    tiles: int
+    n_views: int
+
+    @staticmethod
+    def allocate(slots: int, tiles: int, capacity: int, n_views: int, device) -> "BatchFrame":
+        lib = L.load()
+        s1 = max(slots, 1)
+        kw = dict(device=device)
+        i32 = lambda m: torch.empty(m, dtype=torch.int32, **kw)
+        scratch = int(lib.lumen_gpu_batch_scratch_bytes(s1, capacity, n_views))
+        f = Frame(torch.empty((s1, RECORD_FLOATS), dtype=torch.float32, **kw), i32(s1), i32(s1),
+                  torch.empty(s1, dtype=torch.int64, **kw), [i32(s1), i32(s1)], [i32(s1), i32(s1)],
+                  [i32(capacity), i32(capacity)], [i32(capacity), i32(capacity)],
+                  torch.empty((max(tiles, 1), 2), dtype=torch.int32, **kw),
+                  torch.empty(scratch, dtype=torch.uint8, **kw), capacity)
+        return BatchFrame(f, s1, tiles, n_views)
+
+    def fits(self, slots: int, tiles: int, capacity: int, n_views: int) -> bool:
+        lib = L.load()
+        need = int(lib.lumen_gpu_batch_scratch_bytes(max(slots, 1), self.frame.capacity, n_views))
+        return (self.slots >= slots and self.tiles >= tiles and self.frame.capacity >= capacity
+                and self.frame.scratch.numel() >= need)
+
+
+@dataclass
+class ViewImage:
+    rgb: torch.Tensor            # [H, W, 3]
+    depth: torch.Tensor          # [H, W]
+    alpha: torch.Tensor          # [H, W]
+    n_contrib: torch.Tensor      # [H, W] int32
+    last_idx: torch.Tensor       # [H, W] int32 (offset within the view's sorted instances)
+
+
+@dataclass
+class BatchResult:
+    images: list                 # ViewImage per view
+    n_visible: int
+    n_instances: int
+    sorted_buffer: int
+    tile_begin: list             # batch-wide id of each view's tile 0
+    frame: BatchFrame
+    options: RenderOptions = None
+
+    @property
+    def sorted_keys(self) -> torch.Tensor:
+        """The batch's 64-bit keys ((view tile offset + tile) << 32 | depth
+        key), in sorted order."""
+        lib = L.load()
+        dev = self.images[0].rgb.device
+        out = torch.empty(max(self.n_instances, 1), dtype=torch.int64, device=dev)
+        fs = self.frame.frame.c_struct()
+        opt = L.render_options(self.options or RenderOptions())
+        L.check(lib.lumen_gpu_frame_sorted_keys64(C.byref(fs), C.byref(opt), _p(out), _stream_handle(dev)),
+                "sorted_keys64")
+        return out[: self.n_instances]
+
+    @property
+    def sorted_vals(self) -> torch.Tensor:
+        return self.frame.frame.vals[self.sorted_buffer][: self.n_instances]
+
+
+_batch_capacity_hint = {}
+
+
+def batch_views(views, images) -> "C.Array":
+    """The LumenGpuBatchView array for (Scene, ViewCamera) pairs and their
+    ViewImage outputs."""
+    arr = (L.LumenGpuBatchView * len(views))()
+    for i, ((scene, cam), im) in enumerate(zip(views, images)):
+        arr[i].gaussians = scene.struct
+        arr[i].camera = L.view_camera(cam)
+        img = L.LumenGpuImage()
+        img.rgb, img.depth, img.alpha = _p(im.rgb), _p(im.depth), _p(im.alpha)
+        img.n_contrib, img.last_idx = _p(im.n_contrib), _p(im.last_idx)
+        arr[i].image = img
+    return arr
+
+
+def allocate_images(cameras, device) -> list:
+    out = []
+    for cam in cameras:
+        H, W = int(cam.height), int(cam.width)
+        out.append(ViewImage(torch.empty((H, W, 3), dtype=torch.float32, device=device),
+                             torch.empty((H, W), dtype=torch.float32, device=device),
+                             torch.empty((H, W), dtype=torch.float32, device=device),
+                             torch.empty((H, W), dtype=torch.int32, device=device),
+                             torch.empty((H, W), dtype=torch.int32, device=device)))
+    return out
+
+
+def render_batch(views, options: Optional[RenderOptions] = None, frame: Optional[BatchFrame] = None,
+                 capacity: Optional[int] = None, images: Optional[list] = None) -> BatchResult:
+    """Render several (Scene, ViewCamera) views in one pipeline
+    (lumen_gpu_render_batch). Each view's outputs equal rendering it alone.
+    Waits for the batch (reads the instance count back to check capacity)."""
+    options = options or RenderOptions()
+    lib = L.load()
+    if not views:
+        raise ValueError("render_batch needs at least one view")
+    dev = views[0][0].device
+    images = images or allocate_images([c for _, c in views], dev)
+    arr = batch_views(views, images)
+    nv = len(views)
+    slots, tiles = C.c_int64(0), C.c_int64(0)
+    L.check(lib.lumen_gpu_batch_sizes(arr, nv, C.byref(slots), C.byref(tiles)), "batch_sizes")
+    slots, tiles = int(slots.value), int(tiles.value)
+    key = (slots, tiles, nv)
+    if capacity is None:
+        capacity = _batch_capacity_hint.get(key, max(1 << 16, 8 * slots))
+    if frame is None or not frame.fits(slots, tiles, capacity, nv):
+        frame = BatchFrame.allocate(slots, tiles, capacity, nv, dev)
+    opt = L.render_options(options)
+    stream = _stream_handle(dev)
+    counts = L.LumenGpuCounts()
+    for _ in range(2):
+        fs = frame.frame.c_struct()
+        L.check(lib.lumen_gpu_render_batch(arr, nv, C.byref(opt), C.byref(fs), stream), "render_batch")
+        L.check(lib.lumen_gpu_read_counts(C.byref(fs), C.byref(counts), stream), "read_counts")
+        if not counts.error_flags & L.ERR_CAPACITY:
+            break
+        need = int(counts.n_instances)
+        frame = BatchFrame.allocate(slots, tiles, need + need // 4 + 4096, nv, dev)
+    if counts.error_flags:
+        raise L.LumenError(-4 if not counts.error_flags & L.ERR_CAPACITY else -2,
+                           f"render_batch device flags {counts.error_flags:#x}")
+    _batch_capacity_hint[key] = frame.frame.capacity
+    tile_begin, t = [], 0
+    for _, cam in views:
+        tile_begin.append(t)
+        t += cam.n_tiles
+    return BatchResult(images, int(counts.n_visible), int(counts.n_instances), int(counts.sorted_buffer),
+                       tile_begin, frame, options)
+
+
 def sort_pairs(keys: torch.Tensor, vals: torch.Tensor):
     """Stable sort of (uint64 key, uint32 value) pairs on the device
     (lumen_gpu_sort_pairs). Takes int64/int32 tensors holding the bits;

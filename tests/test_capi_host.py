@@ -17,7 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = []
-    for h in ("lumen.h", "lumen_gpu.h"):
+    for h in ("lumen.h", "lumen_gpu.h", "lumen_serve.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         names += re.findall(r"\b(lumen_\w+)\s*\(", src)
@@ -59,6 +59,37 @@ def test_struct_sizes():
     assert C.sizeof(L.LumenCamera) == 52
     assert C.sizeof(L.LumenViewCamera) == 60
     assert C.sizeof(L.LumenRenderOptions) == 36
+
+
+GPU_STRUCTS = ["LumenGpuGaussians", "LumenViewCamera", "LumenRenderOptions", "LumenSplatRecord", "LumenGpuFrame",
+               "LumenGpuImage", "LumenGpuCounts", "LumenGpuGradients", "LumenGpuBatchView", "LumenServerConfig",
+               "LumenServeResult", "LumenServeStats"]
+
+
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """sizeof and every field offset of the ctypes mirrors equal what a C
+    compiler gives for include/lumen_gpu.h and include/lumen_serve.h."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lumen_serve.h"', "int main(void) {"]
+    for name in GPU_STRUCTS:
+        if not hasattr(L, name):
+            continue
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for field, _ in getattr(L, name)._fields_:
+            lines.append(f'printf("{name}.{field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = dict(line.split() for line in out if line.strip())
+    for name in GPU_STRUCTS:
+        if not hasattr(L, name):
+            continue
+        cls = getattr(L, name)
+        assert int(got[name]) == C.sizeof(cls), name
+        for field, _ in cls._fields_:
+            assert int(got[f"{name}.{field}"]) == getattr(cls, field).offset, f"{name}.{field}"
 
 
 # ---- c_api/test/test_c_api.c:26-44 ----
@@ -137,3 +168,36 @@ def test_rasterize_argument_errors(lib):
     # c_api/src/lumen_c.c:387: NULL arguments are INVALID_ARGUMENT, before any device work
     assert lib.lumen_rasterize(None, None, None, None, None) == -1
     assert lib.lumen_rasterizer_set_config(None, None) == -1
+
+
+def test_server_default_config_and_create_without_device(lib):
+    c = lib.lumen_server_default_config()
+    assert c.max_views_per_batch == 64 and c.max_batches_in_flight == 2 and c.use_graphs == 1
+    assert c.options.tile_size == 16 and c.options.term_mode == 1 and abs(c.options.term_threshold - 0.99) < 1e-7
+    bad = lib.lumen_server_default_config()
+    bad.max_views_per_batch = 0
+    assert not lib.lumen_server_create(C.byref(bad))
+    bad = lib.lumen_server_default_config()
+    bad.autotune, bad.composite_chunk = 0, 100
+    assert not lib.lumen_server_create(C.byref(bad))
+    assert lib.lumen_server_submit(None, 0, None, None, None) == -1
+    assert lib.lumen_server_stats(None, None) == -1
+
+
+def _admit(lib, reqs, max_views=64, caps=(1000, 1000, 1000, 1000)):
+    a = [(C.c_int64 * max(len(reqs), 1))(*[r[i] for r in reqs]) for i in range(4)]
+    return lib.lumen_serve_admit(a[0], a[1], a[2], a[3], len(reqs), max_views, *caps)
+
+
+def test_admission_is_fifo_prefix_within_every_capacity(lib):
+    """The server admits the longest queue prefix whose projection slots,
+    tiles, instance estimates and pixels all fit one slot's buffers."""
+    r = (256, 10, 100, 200)
+    assert _admit(lib, [r] * 3) == 3
+    assert _admit(lib, [r] * 10) == 3          # slots: 4 x 256 > 1000
+    assert _admit(lib, [r] * 10, max_views=2) == 2
+    assert _admit(lib, [(1, 1, 400, 1)] * 5) == 2   # instances
+    assert _admit(lib, [(1, 600, 1, 1)] * 5) == 1   # tiles
+    assert _admit(lib, [(1, 1, 1, 999), (1, 1, 1, 2)]) == 1   # pixels; no skipping ahead
+    assert _admit(lib, [(1001, 1, 1, 1), r]) == 0   # the front request can never fit
+    assert _admit(lib, []) == 0
