@@ -252,7 +252,7 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
                          torch.empty((HEIGHT, WIDTH), device=dev))
     img.rgb, img.depth, img.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
     grads = [torch.empty_like(p) for p in params]
-    splat2d = torch.empty((n, 10), device=dev)
+    splat2d = torch.empty((n, 12), device=dev)
     out = L.LumenGpuGradients()
     out.means, out.scales, out.quats, out.opacities, out.sh = (x.data_ptr() for x in grads)
     out.splat2d = splat2d.data_ptr()
@@ -504,7 +504,7 @@ def serving_leg(dev, n_requests, hbm_budget):
         return lat, time.perf_counter() - t0
 
     out = {}
-    for kind, rate in (("1080p_1M", 2000.0), ("mixed", 2000.0)):
+    for kind, rate in (("1080p_1M", 2000.0), ("1080p_1M", 1400.0), ("mixed", 2000.0), ("mixed", 1400.0)):
         sc_of, cams = workload(kind, n_requests, seed=7 if kind == "mixed" else 8)
         warm_of, warm_cams = workload(kind, max(n_requests // 2, 64), seed=99)
         with serve.Server(work_budget_bytes=hbm_budget, max_views_per_batch=64, max_batches_in_flight=2,
@@ -521,7 +521,7 @@ def serving_leg(dev, n_requests, hbm_budget):
         per_call(sc_of[:min(len(sc_of), 64)], cams[:min(len(cams), 64)])
         pc_lat, pc_wall = per_call(sc_of, cams)
         batches = s1["batches"] - s0["batches"]
-        out[kind] = {
+        out[f"{kind}@{int(rate)}"] = {
             "requests": n_requests, "offered_req_per_s": rate,
             "served_frames_per_s": n_requests / span_s, "served_p50_ms": _percentile(lat, 50),
             "served_p99_ms": _percentile(lat, 99), "mean_batch_views": n_requests / max(batches, 1),
@@ -669,6 +669,10 @@ def main():
             pg.all_reduce(v, op=pg.ReduceOp.MIN)
             e2e["value"] = float(v.item()) * world
         line["e2e"] = e2e
+        if "serving" in line:   # served frames against per-call renders through the drop-in C ABI
+            for k, v in line["serving"].items():
+                if k.startswith("1080p_1M"):
+                    v["served_over_capi_per_call"] = v["served_frames_per_s"] / e2e["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if pg:

@@ -207,6 +207,23 @@ LumenStatus lumen_gpu_render_forward_timed(const LumenGpuGaussians* gaussians, c
 LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms[4], float* total_ms,
                                        int* n_frames);
 
+/* Launch parameters of the forward; none of them changes any output.
+ * composite_chunk: sorted instances the compositor stages per round (128,
+ * 256 or 512); *_sort_items: keys per thread in a digit pass of the depth
+ * and tile sorts (8 or 16, tiles of 2048 or 4096 keys). Defaults 256, 8, 16. */
+typedef struct {
+    int32_t composite_chunk;
+    int32_t depth_sort_items;
+    int32_t tile_sort_items;
+} LumenGpuLaunch;
+
+/* lumen_gpu_render_forward with chosen launch parameters; with a stage
+ * timer (may be NULL) it records stage events like the timed entry point. */
+LumenStatus lumen_gpu_render_forward_ex(const LumenGpuGaussians* gaussians, const LumenViewCamera* camera,
+                                        const LumenRenderOptions* options, const LumenGpuLaunch* launch,
+                                        LumenGpuFrame* frame, LumenGpuImage* image, LumenGpuStageTimer* timer,
+                                        void* stream);
+
 /* ---------------------------------------------------------------- batches
  * Several views rendered by one pipeline: one projection over all views'
  * Gaussians, one depth sort, one tile sort whose 32-bit keys are batch-wide
@@ -255,8 +272,9 @@ LumenStatus lumen_gpu_camera_from_lookat(const LumenCamera* camera, uint32_t wid
  * means [N,3], scales [N,3], quats [N,4], opacities [N], sh [N,48]. When the
  * forward ran with params_are_logits, scales and opacities receive the
  * gradients of the log-scales and the opacity logits. splat2d is a work
- * buffer of N x 10 floats (per-Gaussian gradients of the 2-D splat: centre,
- * conic, opacity, colour, depth), zeroed by the call. */
+ * buffer of N x 12 floats, 16-byte aligned (per-Gaussian gradients of the
+ * 2-D splat: centre, conic, opacity, colour, depth, 2 unused), zeroed by
+ * the call. */
 typedef struct {
     float* means;
     float* scales;

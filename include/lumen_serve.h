@@ -49,7 +49,8 @@ typedef struct {
     int32_t use_graphs;             /* 1: one CUDA graph launch per batch; 0: plain launches */
     int32_t autotune;               /* 1: pick launch parameters per batch class by timing */
     int32_t composite_chunk;        /* fixed choice when autotune is 0: 128, 256 or 512 */
-    int32_t sort_items;             /* fixed choice when autotune is 0: 8 or 16 */
+    int32_t sort_items;             /* fixed choice when autotune is 0: keys per thread of the
+                                       tile sort's digit passes, 8 or 16 (the depth sort uses 8) */
     LumenRenderOptions options;     /* shared by every request */
 } LumenServerConfig;
 
@@ -62,7 +63,7 @@ typedef struct {
     double done_ms;                 /* its bytes were in the host buffer */
     int64_t n_instances;            /* tile instances of this view */
     int32_t composite_chunk;        /* launch parameters of its batch */
-    int32_t sort_items;
+    int32_t sort_items;             /* of the tile sort */
 } LumenServeResult;
 
 typedef struct {
@@ -78,7 +79,7 @@ typedef struct {
 } LumenServeStats;
 
 /* Defaults: 8 GiB budget, 64 views, 2 batches in flight, graphs and
- * autotuning on, chunk 256, 16 items, the reference's render options. */
+ * autotuning on, chunk 256, 16 tile-sort items, alpha >= 0.99 termination. */
 LumenServerConfig lumen_server_default_config(void);
 /* On the current device. NULL on failure (bad config, no device, memory). */
 LumenServer* lumen_server_create(const LumenServerConfig* config);

@@ -98,6 +98,10 @@ class LumenGpuImage(C.Structure):
     _fields_ = [("rgb", _P), ("depth", _P), ("alpha", _P), ("n_contrib", _P), ("last_idx", _P), ("rgb8", _P)]
 
 
+class LumenGpuLaunch(C.Structure):
+    _fields_ = [("composite_chunk", C.c_int32), ("depth_sort_items", C.c_int32), ("tile_sort_items", C.c_int32)]
+
+
 class LumenGpuBatchView(C.Structure):
     _fields_ = [("gaussians", LumenGpuGaussians), ("camera", LumenViewCamera), ("reserved", C.c_int32),
                 ("image", LumenGpuImage)]
@@ -189,6 +193,9 @@ SIGNATURES = {
     "lumen_gpu_render_forward_timed": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenViewCamera),
                                                  C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame),
                                                  C.POINTER(LumenGpuImage), _P, _P]),
+    "lumen_gpu_render_forward_ex": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenViewCamera),
+                                              C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuLaunch),
+                                              C.POINTER(LumenGpuFrame), C.POINTER(LumenGpuImage), _P, _P]),
     "lumen_gpu_batch_sizes": (C.c_int, [C.POINTER(LumenGpuBatchView), C.c_int32, C.POINTER(C.c_int64),
                                         C.POINTER(C.c_int64)]),
     "lumen_gpu_batch_scratch_bytes": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32]),

@@ -50,7 +50,7 @@ class _RenderFunction(torch.autograd.Function):
                  torch.empty_like(logits), torch.empty_like(sh)]
         if n == 0:
             return grads[0], grads[1], grads[2], grads[3], grads[4].reshape(ctx.sh_shape), None, None
-        splat2d = torch.empty((n, 10), dtype=torch.float32, device=dev)
+        splat2d = torch.empty((n, 12), dtype=torch.float32, device=dev)
         out = L.LumenGpuGradients()
         out.means, out.scales, out.quats, out.opacities, out.sh = (g.data_ptr() for g in grads)
         out.splat2d = splat2d.data_ptr()

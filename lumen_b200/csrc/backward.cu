@@ -31,6 +31,7 @@
 namespace lumen {
 
 constexpr int kGrad2D = 10;   /* cx, cy, ic00, ic01, ic11, opacity, r, g, b, depth */
+constexpr int kGrad2DStride = 12;   /* floats per Gaussian in splat2d: 16-byte rows for vector atomics */
 
 struct BackwardSmem {
     float4 geo[kTilePixels];
@@ -161,7 +162,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                 if (power < 0.0f) power = 0.0f;
                 else if (power > 4.5f) skip = true;
                 if (!skip) {
-                    float alpha = gg.w * lumen_expf(-power);
+                    float alpha = gg.w * lumen_expf_core(-power);
                     if (alpha > (float)0.99) alpha = (float)0.99;
                     if (!(alpha < min_alpha())) {
                         T *= (1.0f - alpha);
@@ -215,7 +216,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                 if (power < 0.0f) { power = 0.0f; pclamp = true; }
                 else if (power > 4.5f) skip = true;
                 if (!skip) {
-                    const float gexp = lumen_expf(-power);
+                    const float gexp = lumen_expf_core(-power);
                     const float raw = geo.w * gexp;
                     const bool aclamp = raw > (float)0.99;
                     const float alpha = aclamp ? (float)0.99 : raw;
@@ -261,15 +262,17 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
             }
         }
         __syncthreads();
-        /* one atomic per value per (splat, tile) */
+        /* per (splat, tile): three vector atomics (4 + 4 + 2 values) */
         const int i = cs + tid;
         if (i < re) {
-            float* dst = grad2d + (size_t)s.gid[tid] * kGrad2D;
-#pragma unroll
-            for (int k = 0; k < kGrad2D; ++k) {
-                const float a = s.acc[tid][k];
-                if (a != 0.0f) atomicAdd(dst + k, a);
-            }
+            float* dst = grad2d + (size_t)s.gid[tid] * kGrad2DStride;
+            const float* a = s.acc[tid];
+            if (a[0] != 0.0f || a[1] != 0.0f || a[2] != 0.0f || a[3] != 0.0f)
+                atomicAdd(reinterpret_cast<float4*>(dst), make_float4(a[0], a[1], a[2], a[3]));
+            if (a[4] != 0.0f || a[5] != 0.0f || a[6] != 0.0f || a[7] != 0.0f)
+                atomicAdd(reinterpret_cast<float4*>(dst + 4), make_float4(a[4], a[5], a[6], a[7]));
+            if (a[8] != 0.0f || a[9] != 0.0f)
+                atomicAdd(reinterpret_cast<float2*>(dst + 8), make_float2(a[8], a[9]));
         }
         __syncthreads();
     }
@@ -339,10 +342,12 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
         for (int k = 0; k < 12; ++k) gsh4[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return;
     }
-    const float* G = grad2d + i * 10;
-    const float g_cx = G[0], g_cy = G[1], g_a = G[2], g_b = G[3], g_c = G[4], g_op = G[5];
-    const float g_col[3] = {G[6], G[7], G[8]};
-    const float g_z = G[9];
+    const float4 G0 = reinterpret_cast<const float4*>(grad2d + i * kGrad2DStride)[0];
+    const float4 G1 = reinterpret_cast<const float4*>(grad2d + i * kGrad2DStride)[1];
+    const float2 G2 = reinterpret_cast<const float2*>(grad2d + i * kGrad2DStride)[4];
+    const float g_cx = G0.x, g_cy = G0.y, g_a = G0.z, g_b = G0.w, g_c = G1.x, g_op = G1.y;
+    const float g_col[3] = {G1.z, G1.w, G2.x};
+    const float g_z = G2.y;
 
     /* parameters and activations */
     const float mx = g.means[i * 3], my = g.means[i * 3 + 1], mz = g.means[i * 3 + 2];
@@ -594,7 +599,8 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenVie
         return LUMEN_ERROR_INVALID_ARGUMENT;
     cudaStream_t s = (cudaStream_t)stream;
     Control* ctrl = (Control*)f->scratch;
-    cudaError_t e = cudaMemsetAsync(out->splat2d, 0, (size_t)g->count * kGrad2D * sizeof(float), s);
+    if (((uintptr_t)out->splat2d & 15u) != 0) return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaError_t e = cudaMemsetAsync(out->splat2d, 0, (size_t)g->count * kGrad2DStride * sizeof(float), s);
     if (e != cudaSuccess) return map_cuda(e);
     const int tiles_x = (cam->width + kTile - 1) / kTile;
     const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);

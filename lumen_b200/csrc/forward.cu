@@ -165,14 +165,15 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
         if (ev) cudaEventRecord(ev[1], s);
         launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
                       &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,
-                      lc.sort_items, sms, s);
+                      lc.depth_sort_items, sms, s);
         launch_emit(vt, f, ctrl, emit_lb, L.proj_blocks, persistent, sms, s);
     } else if (ev) {
         cudaEventRecord(ev[1], s);
     }
     /* the tile-sort region holds 4 passes of 2048-key tiles */
     launch_sort32(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort, tile_lb,
-                  2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.sort_items, sms, s);
+                  2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.tile_sort_items, sms,
+                  s);
     if (ev) cudaEventRecord(ev[2], s);
     launch_ranges(f, ctrl, vt, sms, s);
     if (ev) cudaEventRecord(ev[3], s);
@@ -194,8 +195,16 @@ void launch_init(const ScratchLayout& L, unsigned char* base, const BatchHeader*
                                                h, v, v0 != nullptr);
 }
 
+static bool launch_ok(const LaunchConfig& lc) {
+    return (lc.composite_chunk == 128 || lc.composite_chunk == 256 || lc.composite_chunk == 512) &&
+           (lc.depth_sort_items == 8 || lc.depth_sort_items == 16) &&
+           (lc.tile_sort_items == 8 || lc.tile_sort_items == 16);
+}
+
 static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
-                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream) {
+                                LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream,
+                                const LaunchConfig& lc = kDefaultLaunch) {
+    if (!launch_ok(lc)) return LUMEN_ERROR_INVALID_ARGUMENT;
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
     if (!img || (!img->rgb && !img->rgb8) || !frame_ok(f, g->count, true)) return LUMEN_ERROR_INVALID_ARGUMENT;
@@ -220,7 +229,7 @@ static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamer
     v.inst_begin = -1;
     if (ev) cudaEventRecord(ev[0], s);
     launch_init(L, base, &hdr, &v, s);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, ev, s);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s);
     return map_cuda(cudaGetLastError());
 }
 
@@ -309,6 +318,18 @@ LumenStatus lumen_gpu_render_forward(const LumenGpuGaussians* g, const LumenView
                                      const LumenRenderOptions* opt, LumenGpuFrame* f, LumenGpuImage* img,
                                      void* stream) {
     return forward_impl(g, cam, opt, f, img, nullptr, stream);
+}
+
+LumenStatus lumen_gpu_render_forward_ex(const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                        const LumenRenderOptions* opt, const LumenGpuLaunch* launch,
+                                        LumenGpuFrame* f, LumenGpuImage* img, LumenGpuStageTimer* t, void* stream) {
+    if (!launch) return LUMEN_ERROR_INVALID_ARGUMENT;
+    const LaunchConfig lc = {launch->composite_chunk, launch->depth_sort_items, launch->tile_sort_items};
+    if (!t) return forward_impl(g, cam, opt, f, img, nullptr, stream, lc);
+    if (t->next >= t->max_frames) return LUMEN_ERROR_INVALID_ARGUMENT;
+    LumenStatus st = forward_impl(g, cam, opt, f, img, t->ev + (size_t)t->next * 5, stream, lc);
+    if (st == LUMEN_SUCCESS) t->next++;
+    return st;
 }
 
 LumenStatus lumen_gpu_read_counts(const LumenGpuFrame* f, LumenGpuCounts* c, void* stream) {

@@ -46,11 +46,12 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
 namespace {
 
 constexpr int kVariants = 6;
-const LaunchConfig kVariantTable[kVariants] = {{256, 16}, {128, 16}, {512, 16}, {256, 8}, {128, 8}, {512, 8}};
+const LaunchConfig kVariantTable[kVariants] = {{256, 8, 16}, {128, 8, 16}, {512, 8, 16},
+                                                {256, 8, 8},  {128, 8, 8},  {512, 8, 8}};
 
 int variant_of(int chunk, int items) {
     for (int i = 0; i < kVariants; ++i)
-        if (kVariantTable[i].composite_chunk == chunk && kVariantTable[i].sort_items == items) return i;
+        if (kVariantTable[i].composite_chunk == chunk && kVariantTable[i].tile_sort_items == items) return i;
     return -1;
 }
 
@@ -371,7 +372,7 @@ void scheduler_main(LumenServer* srv) {
             r->result.start_ms = t;
             r->result.batch_views = k;
             r->result.composite_chunk = kVariantTable[s->variant].composite_chunk;
-            r->result.sort_items = kVariantTable[s->variant].sort_items;
+            r->result.sort_items = kVariantTable[s->variant].tile_sort_items;
         }
         s->busy = true;
         srv->stats.batches++;

@@ -62,7 +62,8 @@ def test_struct_sizes():
 
 
 GPU_STRUCTS = ["LumenGpuGaussians", "LumenViewCamera", "LumenRenderOptions", "LumenSplatRecord", "LumenGpuFrame",
-               "LumenGpuImage", "LumenGpuCounts", "LumenGpuGradients", "LumenGpuBatchView", "LumenServerConfig",
+               "LumenGpuImage", "LumenGpuCounts", "LumenGpuGradients", "LumenGpuBatchView", "LumenGpuLaunch",
+               "LumenServerConfig",
                "LumenServeResult", "LumenServeStats"]
 
 
