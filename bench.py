@@ -266,7 +266,7 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
                                              stream), "forward")
         L.check(lib.lumen_gpu_l1_loss(rgb.data_ptr(), target.data_ptr(), rgb.numel(), gimg.data_ptr(),
                                       loss.data_ptr(), l1s.data_ptr(), stream), "l1")
-        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs),
+        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs), C.byref(img),
                                               gimg.data_ptr(), None, None, C.byref(out), stream), "backward")
 
     for _ in range(warmup):
@@ -286,7 +286,7 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
     b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     b0.record()
     for _ in range(max(steps // 4, 1)):
-        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs),
+        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs), C.byref(img),
                                               gimg.data_ptr(), None, None, C.byref(out), stream), "backward")
     b1.record()
     torch.cuda.synchronize(dev)

@@ -285,17 +285,22 @@ typedef struct {
 } LumenGpuGradients;
 
 /* Gradients of a scalar loss L through the forward that filled `frame`
- * (same gaussians, camera and options; the frame must not have been reused).
- * grad_rgb [H,W,3] = dL/d rgb is required; grad_depth and grad_alpha
- * ([H,W] each) may be NULL. Per tile, the transmittance is recomputed by a
- * forward sweep and the splats are then visited back to front (no per-splat
- * state is stored by the forward). No counterpart in the reference: it has
- * no analytic backward (src/optim/gradients.mojo:11-106 stores gradients,
- * src/optim/trainer.mojo:61-66 injects placeholders). Does not wait. */
+ * and `forward_image` (same gaussians, camera and options; neither reused
+ * since). forward_image needs rgb and alpha (and depth when grad_depth is
+ * given with compute_depth). grad_rgb [H,W,3] = dL/d rgb is required;
+ * grad_depth and grad_alpha ([H,W] each) may be NULL. Per tile, each
+ * pixel's splats are walked front to back with the forward's arithmetic:
+ * the transmittance before every splat is recomputed (nothing per splat is
+ * stored by the forward) and the colour blended behind a splat is the
+ * forward's output minus the running sum. No counterpart in the reference:
+ * it has no analytic backward (src/optim/gradients.mojo:11-106 stores
+ * gradients, src/optim/trainer.mojo:61-66 injects placeholders). Does not
+ * wait. */
 LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* gaussians, const LumenViewCamera* camera,
                                       const LumenRenderOptions* options, const LumenGpuFrame* frame,
-                                      const float* grad_rgb, const float* grad_depth, const float* grad_alpha,
-                                      LumenGpuGradients* grads, void* stream);
+                                      const LumenGpuImage* forward_image, const float* grad_rgb,
+                                      const float* grad_depth, const float* grad_alpha, LumenGpuGradients* grads,
+                                      void* stream);
 
 /* Mean L1 loss and its subgradient, compute_l1_loss (src/optim/loss.mojo:11-35):
  * loss = mean |pred - target|, grad[i] = +1/n if pred[i] - target[i] >= 0

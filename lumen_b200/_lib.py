@@ -182,8 +182,9 @@ SIGNATURES = {
     "lumen_cloud_append": (C.c_int, [_P, C.POINTER(LumenGaussian), C.c_size_t]),
     "lumen_gpu_sort_pairs_noalloc": (C.c_int, [_P, _P, C.c_int64, _P]),
     "lumen_gpu_render_backward": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenViewCamera),
-                                            C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame), _P, _P, _P,
-                                            C.POINTER(LumenGpuGradients), _P]),
+                                            C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame),
+                                            C.POINTER(LumenGpuImage), _P, _P, _P, C.POINTER(LumenGpuGradients),
+                                            _P]),
     "lumen_gpu_l1_loss_scratch_bytes": (C.c_size_t, []),
     "lumen_gpu_l1_loss": (C.c_int, [_P, _P, C.c_int64, _P, _P, _P, _P]),
     "lumen_gpu_camera_from_lookat": (C.c_int, [C.POINTER(LumenCamera), C.c_uint32, C.c_uint32, C.c_float,

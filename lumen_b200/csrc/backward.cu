@@ -3,20 +3,21 @@
  * counterpart: the reference has no analytic backward; its gradient code
  * only stores buffers, src/optim/gradients.mojo:11-106).
  *
- * K6 composite_backward_kernel: per 16x16 tile, per pixel. A forward sweep
- * recomputes the final transmittance and the last splat each pixel visited
- * (nothing per splat is stored by the forward); a reverse sweep then walks
- * the pixel's splats back to front, recovering T_j = T_{j+1} / (1 - alpha_j)
- * and the suffix colour and depth sums, and forms per splat
+ * K6 composite_backward_kernel: per 16x16 tile, per pixel, one front-to-
+ * back sweep with the forward's own arithmetic: the transmittance T_j
+ * before each splat is recomputed exactly as the forward computed it (so
+ * the sweep stops on the same splat), and the colour and depth blended
+ * after splat j are the forward's outputs minus the prefix sums up to j
+ * (nothing per splat is stored by the forward). Per splat:
  *   dL/dc = G_rgb w, dL/dz = G_depth w,
- *   dL/dalpha = sum_ch G_ch (c_ch T_j - S_ch / (1 - alpha))
- *             + G_depth (z T_j - S_z / (1 - alpha))
+ *   dL/dalpha = sum_ch G_ch (c_ch T_j - (C_ch - P_ch,j) / (1 - alpha))
+ *             + G_depth (z T_j - (D - P_z,j) / (1 - alpha))
  *             + (G_alpha - [white] sum_ch G_ch) T_final / (1 - alpha),
  * then through alpha = min(op exp(-power), 0.99) (no gradient when clamped)
  * and power = 0.5 (a dx^2 + 2 b dx dy + c dy^2) to the centre, the conic and
  * the opacity. The 10 values per splat are reduced over the warp by
  * shuffles, over the CTA in shared memory, and added to the splat's
- * Gaussian with one atomic each per tile.
+ * Gaussian with three vector atomics per tile.
  *
  * K7 project_backward_kernel: per Gaussian, the chain rule through the
  * conic inverse, the EWA product T Sigma T^T with T = J W, the projective
@@ -41,7 +42,6 @@ struct BackwardSmem {
     unsigned short list[kTilePixels / 32][kTilePixels];
     float acc[kTilePixels][kGrad2D];
     unsigned int gid[kTilePixels];
-    int max_last;
 };
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -119,8 +119,10 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
 __global__ void __launch_bounds__(kTilePixels, 4)
 composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, Control* ctrl,
                           int width, int height, int tiles_x, LumenRenderOptions opt,
-                          const float* __restrict__ grad_rgb, const float* __restrict__ grad_depth,
-                          const float* __restrict__ grad_alpha, float* __restrict__ grad2d) {
+                          const float* __restrict__ out_rgb, const float* __restrict__ out_depth,
+                          const float* __restrict__ out_alpha, const float* __restrict__ grad_rgb,
+                          const float* __restrict__ grad_depth, const float* __restrict__ grad_alpha,
+                          float* __restrict__ grad2d) {
     __shared__ BackwardSmem s;
     const int tile = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -145,70 +147,42 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     const float thr = opt.term_threshold;
     const bool mode_alpha = opt.term_mode == 1;
 
-    /* ---- sweep 1: the forward, for the final T and the last splat visited ---- */
-    float T = 1.0f;
-    int last = re - 1;
+    /* the pixel's upstream gradient and the forward's outputs: colour and
+     * depth accumulated over all blended splats, final transmittance */
+    float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, g_a = 0.0f;
+    float C_r = 0.0f, C_g = 0.0f, C_b = 0.0f, C_z = 0.0f, T_final = 1.0f;
+    if (inside) {
+        g_r = grad_rgb[pix * 3 + 0];
+        g_g = grad_rgb[pix * 3 + 1];
+        g_b = grad_rgb[pix * 3 + 2];
+        if (grad_depth && opt.compute_depth) {
+            g_d = grad_depth[pix];
+            C_z = out_depth[pix];
+        }
+        if (grad_alpha) g_a = grad_alpha[pix];
+        T_final = 1.0f - out_alpha[pix];
+        const float bg = opt.white_background ? T_final : 0.0f;
+        C_r = out_rgb[pix * 3 + 0] - bg;
+        C_g = out_rgb[pix * 3 + 1] - bg;
+        C_b = out_rgb[pix * 3 + 2] - bg;
+    }
+    /* terms of dL/dalpha_j that scale with T_final / (1 - alpha_j) */
+    const float g_tail = (g_a - (opt.white_background ? (g_r + g_g + g_b) : 0.0f)) * T_final;
+
+    /* front to back, with the forward's own arithmetic: T and the prefix
+     * sums P are the forward's, so termination falls on the same splat, and
+     * the colour blended after splat j is C - P_j */
+    float T = 1.0f, P_r = 0.0f, P_g = 0.0f, P_b = 0.0f, P_z = 0.0f;
     bool done = !inside;
     for (int cs = rs; cs < re; cs += kTilePixels) {
         if (__syncthreads_count(!done) == 0) break;
         const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, re, tile_x0, tile_y0);
         for (int t = 0; t < cnt; ++t) {
             const int j = s.list[warp][t];
-            if (!done) {
-                const float4 gg = s.geo[j], cc = s.con[j];
-                const float dx = pxc - gg.x, dy = pyc - gg.y;
-                float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
-                bool skip = false;
-                if (power < 0.0f) power = 0.0f;
-                else if (power > 4.5f) skip = true;
-                if (!skip) {
-                    float alpha = gg.w * lumen_expf_core(-power);
-                    if (alpha > (float)0.99) alpha = (float)0.99;
-                    if (!(alpha < min_alpha())) {
-                        T *= (1.0f - alpha);
-                        const float acc = 1.0f - T;
-                        if (mode_alpha ? (acc >= thr) : (T <= thr)) {
-                            done = true;
-                            last = cs + j;
-                        }
-                    }
-                }
-            }
-            if (__all_sync(0xffffffffu, done)) break;
-        }
-        __syncthreads();
-    }
-    if (!inside) last = rs - 1;   /* outside pixels take part in no splat */
-
-    /* ---- sweep 2: back to front ---- */
-    float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, g_a = 0.0f;
-    if (inside) {
-        g_r = grad_rgb[pix * 3 + 0];
-        g_g = grad_rgb[pix * 3 + 1];
-        g_b = grad_rgb[pix * 3 + 2];
-        if (grad_depth && opt.compute_depth) g_d = grad_depth[pix];
-        if (grad_alpha) g_a = grad_alpha[pix];
-    }
-    const float T_final = T;
-    /* terms of dL/dalpha that scale with T_final / (1 - alpha) */
-    const float g_tail = (g_a - (opt.white_background ? (g_r + g_g + g_b) : 0.0f)) * T_final;
-    float S_r = 0.0f, S_g = 0.0f, S_b = 0.0f, S_z = 0.0f;
-    if (tid == 0) s.max_last = rs - 1;
-    __syncthreads();
-    atomicMax(&s.max_last, last);
-    __syncthreads();
-    const int max_last = s.max_last;
-    if (max_last < rs) return;
-    const int top_chunk = rs + ((max_last - rs) / kTilePixels) * kTilePixels;
-    for (int cs = top_chunk; cs >= rs; cs -= kTilePixels) {
-        const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, re, tile_x0, tile_y0);
-        for (int t = cnt - 1; t >= 0; --t) {
-            const int j = s.list[warp][t];
-            const int inst = cs + j;
             float gcx = 0.0f, gcy = 0.0f, ga = 0.0f, gb = 0.0f, gc = 0.0f, gop = 0.0f;
             float gr = 0.0f, gg_ = 0.0f, gbl = 0.0f, gz = 0.0f;
             bool contrib = false;
-            if (inst <= last) {
+            if (!done) {
                 const float4 geo = s.geo[j], cc = s.con[j];
                 const float dx = pxc - geo.x, dy = pyc - geo.y;
                 float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
@@ -223,22 +197,22 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                     if (!(alpha < min_alpha())) {
                         contrib = true;
                         const float4 col = s.col[j];
-                        const float one_m = 1.0f - alpha;
-                        const float Tj = T / one_m;
-                        const float w = alpha * Tj;
+                        const float w = alpha * T;
                         gr = g_r * w;
                         gg_ = g_g * w;
                         gbl = g_b * w;
                         gz = g_d * w;
-                        const float inv = 1.0f / one_m;
-                        const float dalpha = g_r * (col.x * Tj - S_r * inv) + g_g * (col.y * Tj - S_g * inv) +
-                                             g_b * (col.z * Tj - S_b * inv) + g_d * (geo.z * Tj - S_z * inv) +
-                                             g_tail * inv;
-                        S_r += col.x * w;
-                        S_g += col.y * w;
-                        S_b += col.z * w;
-                        S_z += geo.z * w;
-                        T = Tj;
+                        P_r += col.x * w;
+                        P_g += col.y * w;
+                        P_b += col.z * w;
+                        P_z += geo.z * w;
+                        const float inv = __frcp_rn(1.0f - alpha);
+                        const float dalpha = g_r * (col.x * T - (C_r - P_r) * inv) +
+                                             g_g * (col.y * T - (C_g - P_g) * inv) +
+                                             g_b * (col.z * T - (C_b - P_b) * inv) +
+                                             g_d * (geo.z * T - (C_z - P_z) * inv) + g_tail * inv;
+                        T *= (1.0f - alpha);
+                        if (mode_alpha ? (1.0f - T >= thr) : (T <= thr)) done = true;
                         if (!aclamp) {
                             gop = dalpha * gexp;
                             if (!pclamp) {
@@ -260,6 +234,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                 const int k = transposed_index(lane);
                 if ((lane & 1) == 0 && k < kGrad2D && r != 0.0f) atomicAdd(&s.acc[j][k], r);
             }
+            if (__all_sync(0xffffffffu, done)) break;
         }
         __syncthreads();
         /* per (splat, tile): three vector atomics (4 + 4 + 2 values) */
@@ -274,7 +249,6 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
             if (a[8] != 0.0f || a[9] != 0.0f)
                 atomicAdd(reinterpret_cast<float2*>(dst + 8), make_float2(a[8], a[9]));
         }
-        __syncthreads();
     }
 }
 
@@ -587,12 +561,13 @@ LumenStatus map_cuda(cudaError_t e);
 extern "C" {
 
 LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenViewCamera* cam,
-                                      const LumenRenderOptions* opt, const LumenGpuFrame* f, const float* grad_rgb,
-                                      const float* grad_depth, const float* grad_alpha, LumenGpuGradients* out,
-                                      void* stream) {
+                                      const LumenRenderOptions* opt, const LumenGpuFrame* f,
+                                      const LumenGpuImage* fwd, const float* grad_rgb, const float* grad_depth,
+                                      const float* grad_alpha, LumenGpuGradients* out, void* stream) {
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
-    if (!f || !f->scratch || !grad_rgb || !out) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (!f || !f->scratch || !grad_rgb || !out || !fwd || !fwd->rgb || !fwd->alpha) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (grad_depth && opt->compute_depth && !fwd->depth) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (g->count == 0) return LUMEN_SUCCESS;
     if (!out->means || !out->scales || !out->quats || !out->opacities || !out->sh || !out->splat2d ||
         !f->records || !f->visible_ids || !f->radii || !f->ranges || !f->vals[0] || !f->vals[1])
@@ -605,7 +580,8 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenVie
     const int tiles_x = (cam->width + kTile - 1) / kTile;
     const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
     composite_backward_kernel<<<tiles, kTilePixels, 0, s>>>(f->records, *f, ctrl, cam->width, cam->height, tiles_x,
-                                                            *opt, grad_rgb, grad_depth, grad_alpha, out->splat2d);
+                                                            *opt, fwd->rgb, fwd->depth, fwd->alpha, grad_rgb,
+                                                            grad_depth, grad_alpha, out->splat2d);
     const long long nb = (g->count + 255) / 256;
     project_backward_kernel<<<(unsigned int)nb, 256, 0, s>>>(*g, *cam, *opt, f->radii, out->splat2d, *out);
     return map_cuda(cudaGetLastError());
