@@ -260,40 +260,45 @@ __device__ __forceinline__ void rot_from_quat(float w, float x, float y, float z
     R[6] = 2.0f * (x * z - w * y); R[7] = 2.0f * (y * z + w * x); R[8] = 1.0f - 2.0f * (x * x + y * y);
 }
 
-/* gradients of the 16 SH basis functions with respect to the (unit)
- * direction components, for the constants of spherical_harmonics.mojo:17-26 */
-__device__ __forceinline__ void sh_basis_and_grad(float x, float y, float z, float Y[16], float dX[16],
-                                                  float dY[16], float dZ[16]) {
+/* SH basis function k and its gradient with respect to the (unit)
+ * direction components, for the constants of spherical_harmonics.mojo:17-26
+ * (k is a compile-time constant after unrolling). */
+__device__ __forceinline__ void sh_term(int k, float x, float y, float z, float& Y, float& dX, float& dY,
+                                        float& dZ) {
     const float C0 = (float)0.28209479177387814, C1 = (float)0.4886025119029199;
     const float C2_0 = (float)1.0925484305920792, C2_1 = (float)0.31539156525252005;
     const float C2_2 = (float)0.5462742152960396, C3_0 = (float)0.5900435899266435;
     const float C3_1 = (float)2.890611442640554, C3_2 = (float)0.4570457994644658;
     const float C3_3 = (float)0.3731763325901154, C3_4 = (float)1.445305721320277;
     const float xx = x * x, yy = y * y, zz = z * z;
-    Y[0] = C0; dX[0] = 0.0f; dY[0] = 0.0f; dZ[0] = 0.0f;
-    Y[1] = -C1 * y; dX[1] = 0.0f; dY[1] = -C1; dZ[1] = 0.0f;
-    Y[2] = C1 * z; dX[2] = 0.0f; dY[2] = 0.0f; dZ[2] = C1;
-    Y[3] = -C1 * x; dX[3] = -C1; dY[3] = 0.0f; dZ[3] = 0.0f;
-    Y[4] = C2_0 * x * y; dX[4] = C2_0 * y; dY[4] = C2_0 * x; dZ[4] = 0.0f;
-    Y[5] = -C2_0 * y * z; dX[5] = 0.0f; dY[5] = -C2_0 * z; dZ[5] = -C2_0 * y;
-    Y[6] = C2_1 * (2.0f * zz - xx - yy); dX[6] = -2.0f * C2_1 * x; dY[6] = -2.0f * C2_1 * y; dZ[6] = 4.0f * C2_1 * z;
-    Y[7] = -C2_0 * x * z; dX[7] = -C2_0 * z; dY[7] = 0.0f; dZ[7] = -C2_0 * x;
-    Y[8] = C2_2 * (xx - yy); dX[8] = 2.0f * C2_2 * x; dY[8] = -2.0f * C2_2 * y; dZ[8] = 0.0f;
-    Y[9] = -C3_0 * y * (3.0f * xx - yy);
-    dX[9] = -6.0f * C3_0 * x * y; dY[9] = -3.0f * C3_0 * (xx - yy); dZ[9] = 0.0f;
-    Y[10] = C3_1 * x * y * z; dX[10] = C3_1 * y * z; dY[10] = C3_1 * x * z; dZ[10] = C3_1 * x * y;
-    Y[11] = -C3_2 * y * (4.0f * zz - xx - yy);
-    dX[11] = 2.0f * C3_2 * x * y; dY[11] = -C3_2 * (4.0f * zz - xx - 3.0f * yy); dZ[11] = -8.0f * C3_2 * y * z;
-    Y[12] = C3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
-    dX[12] = -6.0f * C3_3 * x * z; dY[12] = -6.0f * C3_3 * y * z; dZ[12] = C3_3 * (6.0f * zz - 3.0f * xx - 3.0f * yy);
-    Y[13] = -C3_2 * x * (4.0f * zz - xx - yy);
-    dX[13] = -C3_2 * (4.0f * zz - 3.0f * xx - yy); dY[13] = 2.0f * C3_2 * x * y; dZ[13] = -8.0f * C3_2 * x * z;
-    Y[14] = C3_4 * z * (xx - yy); dX[14] = 2.0f * C3_4 * x * z; dY[14] = -2.0f * C3_4 * y * z; dZ[14] = C3_4 * (xx - yy);
-    Y[15] = -C3_0 * x * (xx - 3.0f * yy);
-    dX[15] = -3.0f * C3_0 * (xx - yy); dY[15] = 6.0f * C3_0 * x * y; dZ[15] = 0.0f;
+    switch (k) {
+        case 0: Y = C0; dX = 0.0f; dY = 0.0f; dZ = 0.0f; break;
+        case 1: Y = -C1 * y; dX = 0.0f; dY = -C1; dZ = 0.0f; break;
+        case 2: Y = C1 * z; dX = 0.0f; dY = 0.0f; dZ = C1; break;
+        case 3: Y = -C1 * x; dX = -C1; dY = 0.0f; dZ = 0.0f; break;
+        case 4: Y = C2_0 * x * y; dX = C2_0 * y; dY = C2_0 * x; dZ = 0.0f; break;
+        case 5: Y = -C2_0 * y * z; dX = 0.0f; dY = -C2_0 * z; dZ = -C2_0 * y; break;
+        case 6: Y = C2_1 * (2.0f * zz - xx - yy); dX = -2.0f * C2_1 * x; dY = -2.0f * C2_1 * y; dZ = 4.0f * C2_1 * z;
+            break;
+        case 7: Y = -C2_0 * x * z; dX = -C2_0 * z; dY = 0.0f; dZ = -C2_0 * x; break;
+        case 8: Y = C2_2 * (xx - yy); dX = 2.0f * C2_2 * x; dY = -2.0f * C2_2 * y; dZ = 0.0f; break;
+        case 9: Y = -C3_0 * y * (3.0f * xx - yy); dX = -6.0f * C3_0 * x * y; dY = -3.0f * C3_0 * (xx - yy);
+            dZ = 0.0f; break;
+        case 10: Y = C3_1 * x * y * z; dX = C3_1 * y * z; dY = C3_1 * x * z; dZ = C3_1 * x * y; break;
+        case 11: Y = -C3_2 * y * (4.0f * zz - xx - yy); dX = 2.0f * C3_2 * x * y;
+            dY = -C3_2 * (4.0f * zz - xx - 3.0f * yy); dZ = -8.0f * C3_2 * y * z; break;
+        case 12: Y = C3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy); dX = -6.0f * C3_3 * x * z;
+            dY = -6.0f * C3_3 * y * z; dZ = C3_3 * (6.0f * zz - 3.0f * xx - 3.0f * yy); break;
+        case 13: Y = -C3_2 * x * (4.0f * zz - xx - yy); dX = -C3_2 * (4.0f * zz - 3.0f * xx - yy);
+            dY = 2.0f * C3_2 * x * y; dZ = -8.0f * C3_2 * x * z; break;
+        case 14: Y = C3_4 * z * (xx - yy); dX = 2.0f * C3_4 * x * z; dY = -2.0f * C3_4 * y * z;
+            dZ = C3_4 * (xx - yy); break;
+        default: Y = -C3_0 * x * (xx - 3.0f * yy); dX = -3.0f * C3_0 * (xx - yy); dY = 6.0f * C3_0 * x * y;
+            dZ = 0.0f; break;
+    }
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt,
                         const int* __restrict__ radii, const float* __restrict__ grad2d, LumenGpuGradients out) {
     __shared__ DevCamera cam_s;
@@ -415,46 +420,61 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
         const float len = sqrtf(vx * vx + vy * vy + vz * vz);
         const bool dok = len > (float)0.000001;
         const float dx_ = dok ? vx / len : 0.0f, dy_ = dok ? vy / len : 0.0f, dz_ = dok ? vz / len : 0.0f;
-        float Y[16], dX[16], dY[16], dZ[16];
-        sh_basis_and_grad(dx_, dy_, dz_, Y, dX, dY, dZ);
         const int n = opt.sh_degree == 0 ? 1 : opt.sh_degree == 1 ? 4 : opt.sh_degree == 2 ? 9 : 16;
-        float shv[48];
         const float4* sh4 = reinterpret_cast<const float4*>(g.sh + i * 48);
+        /* two streaming passes over the coefficients, 4 at a time (12 floats
+         * = 3 float4): the colour before the clamp (which channels pass a
+         * gradient), then the direction gradient and dL/dsh */
+        float v0 = 0.5f, v1 = 0.5f, v2 = 0.5f;
 #pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            const float4 a = __ldg(sh4 + k);
-            shv[4 * k] = a.x; shv[4 * k + 1] = a.y; shv[4 * k + 2] = a.z; shv[4 * k + 3] = a.w;
-        }
-        float gcol[3];
+        for (int grp = 0; grp < 4; ++grp) {
+            if (4 * grp >= n) break;
+            const float4 a = __ldg(sh4 + 3 * grp), b = __ldg(sh4 + 3 * grp + 1), c = __ldg(sh4 + 3 * grp + 2);
+            const float e[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-            float v = 0.5f;
-#pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if (k < n) v += shv[k * 3 + ch] * Y[k];
-            gcol[ch] = (v < 0.0f || v > 1.0f) ? 0.0f : g_col[ch];
-        }
-        float gd0 = 0.0f, gd1 = 0.0f, gd2 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            if (k < n) {
-                const float a = gcol[0] * shv[k * 3] + gcol[1] * shv[k * 3 + 1] + gcol[2] * shv[k * 3 + 2];
-                gd0 += a * dX[k];
-                gd1 += a * dY[k];
-                gd2 += a * dZ[k];
+            for (int kk = 0; kk < 4; ++kk) {
+                const int k = 4 * grp + kk;
+                if (k < n) {
+                    float Y, dX, dY, dZ;
+                    sh_term(k, dx_, dy_, dz_, Y, dX, dY, dZ);
+                    v0 += e[3 * kk] * Y;
+                    v1 += e[3 * kk + 1] * Y;
+                    v2 += e[3 * kk + 2] * Y;
+                }
             }
         }
-        /* dL/dsh[k][ch] = gcol[ch] Y_k, written as 12 float4 */
+        const float gc0 = (v0 < 0.0f || v0 > 1.0f) ? 0.0f : g_col[0];
+        const float gc1 = (v1 < 0.0f || v1 > 1.0f) ? 0.0f : g_col[1];
+        const float gc2 = (v2 < 0.0f || v2 > 1.0f) ? 0.0f : g_col[2];
+        float gd0 = 0.0f, gd1 = 0.0f, gd2 = 0.0f;
         float4* gsh4 = reinterpret_cast<float4*>(gsh);
 #pragma unroll
-        for (int q = 0; q < 12; ++q) {
-            float e[4];
+        for (int grp = 0; grp < 4; ++grp) {
+            float o[12];
+            if (4 * grp < n) {
+                const float4 a = __ldg(sh4 + 3 * grp), b = __ldg(sh4 + 3 * grp + 1), c = __ldg(sh4 + 3 * grp + 2);
+                const float e[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int m = 4 * q + r, k = m / 3, ch = m % 3;
-                e[r] = k < n ? gcol[ch] * Y[k] : 0.0f;
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int k = 4 * grp + kk;
+                    float Y = 0.0f, dX = 0.0f, dY = 0.0f, dZ = 0.0f;
+                    if (k < n) sh_term(k, dx_, dy_, dz_, Y, dX, dY, dZ);
+                    const float s3 = gc0 * e[3 * kk] + gc1 * e[3 * kk + 1] + gc2 * e[3 * kk + 2];
+                    gd0 += s3 * dX;
+                    gd1 += s3 * dY;
+                    gd2 += s3 * dZ;
+                    /* dL/dsh[k][ch] = gcol[ch] Y_k */
+                    o[3 * kk] = gc0 * Y;
+                    o[3 * kk + 1] = gc1 * Y;
+                    o[3 * kk + 2] = gc2 * Y;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 12; ++q) o[q] = 0.0f;
             }
-            gsh4[q] = make_float4(e[0], e[1], e[2], e[3]);
+            gsh4[3 * grp] = make_float4(o[0], o[1], o[2], o[3]);
+            gsh4[3 * grp + 1] = make_float4(o[4], o[5], o[6], o[7]);
+            gsh4[3 * grp + 2] = make_float4(o[8], o[9], o[10], o[11]);
         }
         if (dok) {
             const float dot = gd0 * dx_ + gd1 * dy_ + gd2 * dz_;

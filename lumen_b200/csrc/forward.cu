@@ -33,7 +33,8 @@ void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, uns
                  long long n_blocks, bool persistent, int num_sms, cudaStream_t st);
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
                    SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
-                   const long long* n_range_tiles, unsigned int* err, int items, int num_sms, cudaStream_t st);
+                   const long long* n_range_tiles, unsigned int* err, int items, int key_bytes, int num_sms,
+                   cudaStream_t st);
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
                    long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
                    int num_sms, cudaStream_t st);
@@ -165,15 +166,19 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
         if (ev) cudaEventRecord(ev[1], s);
         launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
                       &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,
-                      lc.depth_sort_items, sms, s);
+                      lc.depth_sort_items, 4, sms, s);
         launch_emit(vt, f, ctrl, emit_lb, L.proj_blocks, persistent, sms, s);
     } else if (ev) {
         cudaEventRecord(ev[1], s);
     }
-    /* the tile-sort region holds 4 passes of 2048-key tiles */
+    /* the tile-sort region holds 4 passes of 2048-key tiles; tile ids below
+     * n_tiles (the batch's, or the bound a persistent launch is sized for)
+     * vary in their low ceil(log2(n_tiles) / 8) bytes only */
+    int tile_bytes = 0;
+    for (long long t = n_tiles - 1; t > 0; t >>= 8) ++tile_bytes;
     launch_sort32(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort, tile_lb,
-                  2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.tile_sort_items, sms,
-                  s);
+                  2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.tile_sort_items,
+                  tile_bytes, sms, s);
     if (ev) cudaEventRecord(ev[2], s);
     launch_ranges(f, ctrl, vt, sms, s);
     if (ev) cudaEventRecord(ev[3], s);

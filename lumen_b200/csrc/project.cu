@@ -7,7 +7,8 @@
  * indices in Gaussian order (pipeline.mojo:141-149) and each appends one
  * key per covered tile (:152-157); the keys are then stably sorted (:166).
  *
- * K1: a block of 256 threads projects 256 consecutive Gaussians and scans
+ * K1: a block of 256 threads projects 256 consecutive Gaussians (their SH
+ * coefficients staged in shared memory by asynchronous copies) and scans
  * their visibility flags; the global offset comes from a decoupled look-back
  * over blocks taken in ticket order, so visible indices are exactly the
  * reference's sequential ones. Each visible splat writes its 48-byte record,
@@ -110,6 +111,7 @@ __global__ void __launch_bounds__(kProjThreads)
 project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOptions opt, LumenGpuFrame f,
                Control* ctrl, unsigned long long* lb) {
     __shared__ ProjSmem s;
+    extern __shared__ float4 sh_stage[];   /* kProjThreads x 12: the block's SH coefficients */
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n_views = n_views_hint > 0 ? n_views_hint : vt->hdr.n_views;
     const long long total_blocks = vt->hdr.total_blocks;
@@ -137,19 +139,38 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
             __syncthreads();
         }
         const long long slot = (long long)blk * kProjThreads + tid;
-        const long long i = (long long)(blk - s.vd.block_begin) * kProjThreads + tid;
+        const long long i0 = (long long)(blk - s.vd.block_begin) * kProjThreads;
+        const long long i = i0 + tid;
+        const long long count = s.vd.g.count;
+        /* the block's SH rows (192 B per Gaussian, contiguous) go to shared
+         * memory with coalesced 16-byte asynchronous copies, overlapped with
+         * the loads of the other parameters */
+        {
+            const int nblk = (int)(count - i0 < kProjThreads ? count - i0 : kProjThreads);
+            const float4* src = reinterpret_cast<const float4*>(s.vd.g.sh + i0 * 48);
+            for (int c = tid; c < nblk * 12; c += kProjThreads) cp_async16(sh_stage + c, src + c);
+            cp_async_commit();
+        }
+        float mx = 0.0f, my = 0.0f, mz = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f, op = 0.0f;
+        float4 q = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+        if (i < count) {
+            const LumenGpuGaussians& g = s.vd.g;
+            const float* m = g.means + i * 3;
+            const float* sc = g.scales + i * 3;
+            q = __ldg(reinterpret_cast<const float4*>(g.quats) + i);
+            mx = __ldg(m); my = __ldg(m + 1); mz = __ldg(m + 2);
+            sx = __ldg(sc); sy = __ldg(sc + 1); sz = __ldg(sc + 2);
+            op = __ldg(g.opacities + i);
+        }
+        cp_async_wait_all();
+        __syncthreads();
 
         Projected p;
         p.visible = false;
         p.radius = 0;
-        if (i < s.vd.g.count) {
-            const LumenGpuGaussians& g = s.vd.g;
-            const float* m = g.means + i * 3;
-            const float* sc = g.scales + i * 3;
-            const float4 q = __ldg(reinterpret_cast<const float4*>(g.quats) + i);
-            p = project_gaussian(s.vd.dcam, __ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(sc), __ldg(sc + 1),
-                                 __ldg(sc + 2), Quat{q.x, q.y, q.z, q.w}, __ldg(g.opacities + i),
-                                 g.sh + i * 48, opt);
+        if (i < count) {
+            p = project_gaussian(s.vd.dcam, mx, my, mz, sx, sy, sz, Quat{q.x, q.y, q.z, q.w}, op,
+                                 reinterpret_cast<const float*>(sh_stage + tid * 12), opt);
             if (f.radii) f.radii[slot] = p.visible ? p.radius : 0;
         }
         unsigned int block_vis = 0;
@@ -314,19 +335,23 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
     }
 }
 
-static int resident_ctas(const void* kernel, int threads) {
+static int resident_ctas(const void* kernel, int threads, size_t smem) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm <= 0)
         per_sm = 1;
     return per_sm;
 }
 
 static int g_project_per_sm = 0, g_emit_per_sm = 0;
+constexpr size_t kProjStageBytes = (size_t)kProjThreads * 48 * sizeof(float);
 
-/* Occupancy of the persistent kernels, queried once (before any capture). */
+/* Kernel attributes and the occupancy of the persistent kernels, set and
+ * queried once (before any capture). */
 void prime_persistent_launches() {
-    g_project_per_sm = resident_ctas((const void*)project_kernel<true>, kProjThreads);
-    g_emit_per_sm = resident_ctas((const void*)emit_kernel<true>, kProjThreads);
+    cudaFuncSetAttribute(project_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kProjStageBytes);
+    cudaFuncSetAttribute(project_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kProjStageBytes);
+    g_project_per_sm = resident_ctas((const void*)project_kernel<true>, kProjThreads, kProjStageBytes);
+    g_emit_per_sm = resident_ctas((const void*)emit_kernel<true>, kProjThreads, 0);
 }
 
 /* Plain launches: one CTA per block (n_blocks known on the host).
@@ -337,9 +362,10 @@ void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& 
     if (n_blocks <= 0) return;
     if (persistent) {
         const int per_sm = g_project_per_sm > 0 ? g_project_per_sm : 1;
-        project_kernel<true><<<per_sm * num_sms, kProjThreads, 0, st>>>(vt, n_views, opt, f, ctrl, lb);
+        project_kernel<true><<<per_sm * num_sms, kProjThreads, kProjStageBytes, st>>>(vt, n_views, opt, f, ctrl, lb);
     } else {
-        project_kernel<false><<<(unsigned int)n_blocks, kProjThreads, 0, st>>>(vt, n_views, opt, f, ctrl, lb);
+        project_kernel<false><<<(unsigned int)n_blocks, kProjThreads, kProjStageBytes, st>>>(vt, n_views, opt, f,
+                                                                                             ctrl, lb);
     }
 }
 

@@ -39,55 +39,64 @@ __device__ __forceinline__ long long sort_count(const SortControl* c, long long 
 }
 
 /* Histogram of every varying digit; clears the look-back regions of the
- * passes that will run; optionally fills the tile ranges with -1. */
-/* One key's varying digits into a warp's private histograms. Consecutive
- * keys often share digits (the instances of one splat), so equal digits
- * within the warp are combined with match_any before the shared add. */
-template <typename KeyT, int kBytes>
-__device__ __forceinline__ void count_key(unsigned int (*h)[256], KeyT k, bool valid, unsigned int varying,
-                                          int lane) {
-#pragma unroll
-    for (int d = 0; d < kBytes; ++d) {
-        if (!(varying & (1u << d))) continue;
-        const unsigned int b = valid ? (unsigned int)((k >> (8 * d)) & 0xFF) : (0x100u + lane);
-        const unsigned int peers = __match_any_sync(0xffffffffu, b);
-        if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d][b], (unsigned int)__popc(peers));
-    }
-}
-
+ * passes that will run; optionally fills the tile ranges with -1.
+ *
+ * Each thread counts runs of kRun consecutive keys: equal digits in a row
+ * are summed in a register and added to the warp's shared histogram once
+ * per run. Tile ids in emission order form long runs in their high byte
+ * (the instances of one splat row), so those collapse to a few atomics;
+ * random digits cost one shared atomic per key, with no warp-wide match. */
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
 histogram_kernel(const KeyT* __restrict__ keys, long long capacity, SortControl* sc, unsigned int* lb,
                  long long lb_tiles_cap, int tile_keys, int* ranges, const long long* n_range_tiles) {
     constexpr int kBytes = (int)sizeof(KeyT);
+    constexpr int kRun = kBytes == 8 ? 8 : 16;           /* 64 bytes of keys per thread and run */
     /* a histogram set per warp (per pair of warps for 8-byte keys, to stay
      * within 32 KB) so warps do not contend on the same shared bins */
     constexpr int kWarps = kBytes == 8 ? 4 : 8;
     __shared__ unsigned int h[kWarps][kBytes][256];
-    const int tid = threadIdx.x, lane = tid & 31, warp = (tid >> 5) % kWarps;
+    const int tid = threadIdx.x, warp = (tid >> 5) % kWarps;
     const long long K = sort_count(sc, capacity);
     const unsigned int varying = K > 1 ? varying_digits(sc, kBytes) : 0u;
     for (int j = tid; j < kWarps * kBytes * 256; j += 256) (&h[0][0][0])[j] = 0u;
     __syncthreads();
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     const long long gtid = (long long)blockIdx.x * blockDim.x + tid;
+    const bool vec = ((uintptr_t)keys & 15u) == 0;   /* runs start 64-byte apart from the base */
     if (varying) {
-        /* 4 consecutive keys per lane and iteration; warps stay in lockstep */
-        const long long nwarps_total = nthreads / 32;
-        const long long gwarp = gtid / 32;
-        for (long long base = gwarp * 128; base < K; base += nwarps_total * 128) {
-            KeyT kk[4];
-            bool ok[4];
+        for (long long c = gtid; c * kRun < K; c += nthreads) {
+            const long long i0 = c * kRun;
+            KeyT k[kRun];
+            const int nk = (int)(K - i0 < kRun ? K - i0 : kRun);
+            if (nk == kRun && vec) {
+                const uint4* src = reinterpret_cast<const uint4*>(keys + i0);
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const long long i = base + r * 32 + lane;
-                ok[r] = i < K;
-                kk[r] = ok[r] ? keys[i] : (KeyT)0;
+                for (int q = 0; q < kRun * kBytes / 16; ++q) {
+                    const uint4 v = src[q];
+                    reinterpret_cast<uint4*>(k)[q] = v;
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < kRun; ++r) k[r] = r < nk ? keys[i0 + r] : (KeyT)0;
             }
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                count_key<KeyT, kBytes>(h[warp], kk[r], ok[r], varying, lane);
-                __syncwarp();
+            for (int d = 0; d < kBytes; ++d) {
+                if (!(varying & (1u << d))) continue;
+                unsigned int prev = (unsigned int)((k[0] >> (8 * d)) & 0xFF), run = 1;
+#pragma unroll
+                for (int r = 1; r < kRun; ++r) {
+                    if (r >= nk) break;
+                    const unsigned int b = (unsigned int)((k[r] >> (8 * d)) & 0xFF);
+                    if (b == prev) {
+                        ++run;
+                    } else {
+                        atomicAdd(&h[warp][d][prev], run);
+                        prev = b;
+                        run = 1;
+                    }
+                }
+                atomicAdd(&h[warp][d][prev], run);
             }
         }
     }
@@ -371,16 +380,20 @@ __global__ void sorted_keys64_kernel(const unsigned int* k0, const unsigned int*
     }
 }
 
+/* key_bytes: the low bytes that can vary at all (a pass per byte is
+ * launched; among those, passes over bytes that turn out constant exit at
+ * once). */
 template <typename KeyT, int kItems>
 void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                       unsigned int* lb, long long lb_tiles_cap, int* ranges, const long long* n_range_tiles,
-                      unsigned int* err, int num_sms, cudaStream_t st) {
+                      unsigned int* err, int key_bytes, int num_sms, cudaStream_t st) {
     histogram_kernel<KeyT><<<num_sms * 4, 256, 0, st>>>(k0, capacity, sc, lb, lb_tiles_cap, kSortThreads * kItems,
                                                         ranges, n_range_tiles);
     const size_t smem = sizeof(PassSmem<KeyT, kItems>);
     /* matches __launch_bounds__: all CTAs resident */
     const int ctas_per_sm = sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : 3) : 2;
-    for (int d = 0; d < (int)sizeof(KeyT); ++d)
+    const int nd = key_bytes < (int)sizeof(KeyT) ? key_bytes : (int)sizeof(KeyT);
+    for (int d = 0; d < nd; ++d)
         onesweep_pass_kernel<KeyT, kItems><<<num_sms * ctas_per_sm, kSortThreads, smem, st>>>(
             k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d);
 }
@@ -389,20 +402,21 @@ void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lo
  * keys); lb_tiles_cap must hold ceil(capacity / (256 * items)) tiles. */
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
                    SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
-                   const long long* n_range_tiles, unsigned int* err, int items, int num_sms, cudaStream_t st) {
+                   const long long* n_range_tiles, unsigned int* err, int items, int key_bytes, int num_sms,
+                   cudaStream_t st) {
     if (items == 8)
         launch_sort_impl<unsigned int, 8>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles, err,
-                                          num_sms, st);
+                                          key_bytes, num_sms, st);
     else
         launch_sort_impl<unsigned int, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles,
-                                           err, num_sms, st);
+                                           err, key_bytes, num_sms, st);
 }
 
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
                    long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
                    int num_sms, cudaStream_t st) {
     launch_sort_impl<unsigned long long, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
-                                             num_sms, st);
+                                             8, num_sms, st);
 }
 
 void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st) {

@@ -274,7 +274,8 @@ struct Projected {
 };
 
 /* SHBasis.evaluate + evaluate_sh_color, spherical_harmonics.mojo:68-111,133-172;
- * sh points at the Gaussian's 48 coefficients. */
+ * sh points at the Gaussian's 48 coefficients (16-byte aligned; the
+ * projection kernel stages them in shared memory). */
 __device__ __forceinline__ void sh_color(const float* __restrict__ sh, float dx0, float dy0, float dz0,
                                          int degree, float& r, float& g, float& b) {
     const float C0 = (float)0.28209479177387814, C1 = (float)0.4886025119029199;
@@ -312,7 +313,7 @@ __device__ __forceinline__ void sh_color(const float* __restrict__ sh, float dx0
     float c[48];
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-        float4 v = __ldg(s4 + k);
+        float4 v = s4[k];
         c[4 * k + 0] = v.x; c[4 * k + 1] = v.y; c[4 * k + 2] = v.z; c[4 * k + 3] = v.w;
     }
     float rr = 0.5f, gg = 0.5f, bb = 0.5f;
@@ -449,6 +450,14 @@ __device__ __forceinline__ unsigned int depth_key(float z, int key_mode) {
 }
 
 /* ------------------------------------------------------------- helpers -- */
+
+/* 16-byte asynchronous copy global -> shared (bypassing L1), and its waits. */
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned int dst = (unsigned int)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ unsigned int lanemask_lt() {
     unsigned int m;
