@@ -122,6 +122,27 @@ class ClockSampler:
                 "samples": len(self.sm), "source": "nvml, 10 ms"}
 
 
+def replica_throughput(ms_per_step, world, pg, dev):
+    """Independent replicas, one per rank: the step time is the slowest
+    rank's (max over ranks) and the whole-job rate is world steps per that
+    time. Returns (max ms per step, steps/s of the job)."""
+    import torch
+    t = torch.tensor([float(ms_per_step)], device=dev)
+    if pg is not None and world > 1:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return ms_max, world * 1000.0 / ms_max
+
+
+def replica_rate(rate, world, pg, dev):
+    """A per-rank rate to the job's: the slowest rank's rate times world."""
+    import torch
+    t = torch.tensor([float(rate)], device=dev)
+    if pg is not None and world > 1:
+        pg.all_reduce(t, op=pg.ReduceOp.MIN)
+    return float(t.item()) * world
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -621,11 +642,7 @@ def main():
     steps = args.steps
     # first-to-last event span over the K back-to-back frames (gaps included)
     ms = total.value / steps
-    ms_t = torch.tensor([ms], device=dev)
-    if pg:
-        pg.all_reduce(ms_t, op=pg.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * 1000.0 / ms_max
+    ms_max, value = replica_throughput(ms, world, pg, dev)
 
     stage_ms = [x / steps for x in stage]
     names = ["project", "sort", "tile_ranges", "composite"]
@@ -665,9 +682,7 @@ def main():
     if not args.no_e2e:
         e2e = e2e_rasterize(sc, scales, opac, steps, args.warmup)
         if pg:   # replicas: the slowest rank's rate times the number of ranks
-            v = torch.tensor([e2e["value"]], device=dev)
-            pg.all_reduce(v, op=pg.ReduceOp.MIN)
-            e2e["value"] = float(v.item()) * world
+            e2e["value"] = replica_rate(e2e["value"], world, pg, dev)
         line["e2e"] = e2e
         if "serving" in line:   # served frames against per-call renders through the drop-in C ABI
             for k, v in line["serving"].items():

@@ -203,7 +203,7 @@ void launch_init(const ScratchLayout& L, unsigned char* base, const BatchHeader*
 static bool launch_ok(const LaunchConfig& lc) {
     return (lc.composite_chunk == 128 || lc.composite_chunk == 256 || lc.composite_chunk == 512) &&
            (lc.depth_sort_items == 8 || lc.depth_sort_items == 16) &&
-           (lc.tile_sort_items == 8 || lc.tile_sort_items == 16);
+           (lc.tile_sort_items == 8 || lc.tile_sort_items == 16 || lc.tile_sort_items == 24);
 }
 
 static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,

@@ -163,7 +163,7 @@ __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, i
 
 /* kItems keys per thread: tiles of 256 * kItems keys. */
 template <typename KeyT, int kItems>
-__global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : 3) : 2)
+__global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : kItems <= 16 ? 3 : 2) : 2)
 onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                      unsigned int* lb_all, long long lb_tiles_cap, unsigned int* err, int digit) {
     constexpr int kTileKeys = kSortThreads * kItems;
@@ -391,15 +391,16 @@ void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lo
                                                         ranges, n_range_tiles);
     const size_t smem = sizeof(PassSmem<KeyT, kItems>);
     /* matches __launch_bounds__: all CTAs resident */
-    const int ctas_per_sm = sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : 3) : 2;
+    const int ctas_per_sm = sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : kItems <= 16 ? 3 : 2) : 2;
     const int nd = key_bytes < (int)sizeof(KeyT) ? key_bytes : (int)sizeof(KeyT);
     for (int d = 0; d < nd; ++d)
         onesweep_pass_kernel<KeyT, kItems><<<num_sms * ctas_per_sm, kSortThreads, smem, st>>>(
             k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d);
 }
 
-/* items: keys per thread of a digit pass, 8 or 16 (tiles of 2048 or 4096
- * keys); lb_tiles_cap must hold ceil(capacity / (256 * items)) tiles. */
+/* items: keys per thread of a digit pass, 8, 16 or 24 (tiles of 2048, 4096
+ * or 6144 keys); lb_tiles_cap must hold ceil(capacity / (256 * items))
+ * tiles. */
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
                    SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
                    const long long* n_range_tiles, unsigned int* err, int items, int key_bytes, int num_sms,
@@ -407,6 +408,9 @@ void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigne
     if (items == 8)
         launch_sort_impl<unsigned int, 8>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles, err,
                                           key_bytes, num_sms, st);
+    else if (items == 24)
+        launch_sort_impl<unsigned int, 24>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles,
+                                           err, key_bytes, num_sms, st);
     else
         launch_sort_impl<unsigned int, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, ranges, n_range_tiles,
                                            err, key_bytes, num_sms, st);
@@ -439,6 +443,8 @@ void configure_sort_kernels() {
                          (int)sizeof(PassSmem<unsigned int, 8>));
     cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(PassSmem<unsigned int, 16>));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned int, 24>));
     cudaFuncSetAttribute(onesweep_pass_kernel<unsigned long long, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(PassSmem<unsigned long long, 16>));
 }
