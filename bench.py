@@ -180,7 +180,57 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def _reference_c_rasterize(sc, scales, opac, n_sample):
+    """The reference's own C renderer (c_api/src/lumen_c.c, built by
+    oracle/Makefile into oracle/_ref/) on the first n_sample Gaussians of the
+    workload at 1080p: seconds per frame, or None when it was not built. A
+    different algorithm from the Mojo path (isotropic, DC-only, qsort)."""
+    import numpy as np
+    from lumen_b200 import _lib as L
+    path = os.path.join(ROOT, "oracle", "_ref", "liblumen_ref.so")
+    if not os.path.exists(path):
+        return None
+    ref = C.CDLL(path)
+    for name in ("lumen_cloud_create", "lumen_cloud_destroy", "lumen_cloud_add_gaussian", "lumen_framebuffer_create",
+                 "lumen_framebuffer_destroy", "lumen_rasterizer_create", "lumen_rasterizer_destroy",
+                 "lumen_rasterize", "lumen_default_config"):
+        res, args = L.SIGNATURES[name]
+        fn = getattr(ref, name)
+        fn.restype, fn.argtypes = res, args
+    n = n_sample
+    aos = np.zeros((n, 59), np.float32)
+    aos[:, 0:3] = sc.means[:n]
+    aos[:, 3:6] = scales[:n]
+    aos[:, 6:10] = sc.quats[:n]
+    aos[:, 10] = opac[:n]
+    aos[:, 11:59] = sc.sh[:n].reshape(n, 48)
+    cloud = ref.lumen_cloud_create(n)
+    gs = (L.LumenGaussian * n).from_buffer_copy(aos.tobytes())
+    for i in range(n):
+        ref.lumen_cloud_add_gaussian(cloud, C.byref(gs[i]))
+    cfg = ref.lumen_default_config()
+    cfg.image_width, cfg.image_height = WIDTH, HEIGHT
+    r = ref.lumen_rasterizer_create(C.byref(cfg))
+    fb = ref.lumen_framebuffer_create(WIDTH, HEIGHT)
+    cam = L.LumenCamera()
+    cam.position, cam.target, cam.up = L.LumenVec3(0, 0, 0), L.LumenVec3(0, 0, 8), L.LumenVec3(0, 1, 0)
+    cam.fov_x_degrees, cam.fov_y_degrees = 50.0 * WIDTH / HEIGHT, 50.0
+    cam.near_plane, cam.far_plane = 0.01, 1000.0
+    st = L.LumenStats()
+    t0 = time.perf_counter()
+    rc = ref.lumen_rasterize(r, cloud, C.byref(cam), fb, C.byref(st))
+    dt = time.perf_counter() - t0
+    ref.lumen_framebuffer_destroy(fb)
+    ref.lumen_rasterizer_destroy(r)
+    ref.lumen_cloud_destroy(cloud)
+    return dt if rc == 0 else None
+
+
 def cpu_baseline():
+    """The oracle restatement of the reference path on the host: all threads
+    (the reported value) and one thread (the reference's scalar execution),
+    one full config-1 frame each; and the reference's own C renderer on a
+    bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from lumen_b200 import scenes
@@ -192,8 +242,23 @@ def cpu_baseline():
     t0 = time.perf_counter()
     O.render(sc.means, s, sc.quats, op, sc.sh, cam, RenderOptions(term_mode=1), stages=False, nthreads=nt)
     dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": UNIT, "cores": nt, "kind": "port",
-            "sample": "one full 1080p frame of config 1 (1M Gaussians), oracle on all host threads"}
+    t0 = time.perf_counter()
+    O.render(sc.means, s, sc.quats, op, sc.sh, cam, RenderOptions(term_mode=1), stages=False, nthreads=1)
+    dt1 = time.perf_counter() - t0
+    out = {"value": 1.0 / dt, "unit": UNIT, "cores": nt, "kind": "port",
+           "sample": "one full 1080p frame of config 1 (1M Gaussians), oracle on all host threads",
+           "single_thread": {"value": 1.0 / dt1, "unit": UNIT, "cores": 1,
+                             "sample": "one full 1080p frame of config 1, oracle on one thread"}}
+    n_sample = 200_000
+    dtr = _reference_c_rasterize(sc, s, op, n_sample)
+    if dtr is not None:
+        scale = N_GAUSSIANS / n_sample
+        out["reference_c_abi"] = {
+            "value": 1.0 / (dtr * scale), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"lumen_rasterize of the reference C library on the first {n_sample} Gaussians at 1080p "
+                      f"({dtr:.2f} s), scaled by {scale:.0f} to a 1M frame; a different algorithm "
+                      "(isotropic, DC-only, qsort) from the Mojo path"}
+    return out
 
 
 def e2e_rasterize(sc, scales, opac, steps, warmup):

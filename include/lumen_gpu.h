@@ -243,10 +243,10 @@ typedef struct {
 } LumenGpuBatchView;
 
 /* Buffer lengths a batch needs: slots = sum over views of count rounded up
- * to 256 (length of records, visible_ids, radii, rects, depth_keys,
- * depth_order; radii may be NULL in a batch frame, else radii[slot] with
- * slot = 256 * (the view's first block) + i), tiles = sum over views of
- * their tiles (ranges holds 2 * tiles). */
+ * to a multiple of 128 (length of records, visible_ids, radii, rects,
+ * depth_keys, depth_order; radii may be NULL in a batch frame, else
+ * radii[slot] with slot = the slots of the views before + i), tiles = sum
+ * over views of their tiles (ranges holds 2 * tiles). */
 LumenStatus lumen_gpu_batch_sizes(const LumenGpuBatchView* views, int32_t n_views, int64_t* slots, int64_t* tiles);
 size_t lumen_gpu_batch_scratch_bytes(int64_t slots, int64_t instance_capacity, int32_t n_views);
 /* Enqueue a batch on `stream` (no host sync; the view list is copied before

@@ -62,8 +62,9 @@ LUMEN_HD int lumen_float_bits(float f) {
 #endif
 }
 
-/* The reduction and polynomial: p = e^r and ki with e^x = p * 2^ki. */
-LUMEN_HD float lumen_expf_reduced(float x, int* ki_out) {
+/* The reduction and polynomial: p = e^r and ki with e^x = p * 2^ki; also
+ * the bits of t = x*log2(e) + 1.5*2^23, which are 0x4B400000 + ki. */
+LUMEN_HD float lumen_expf_reduced(float x, int* ki_out, uint32_t* tbits_out) {
     /* ln 2 = LN2_HI + LN2_LO; LN2_HI = 0x3F317200 has 16 significant bits. */
     const float LN2_HI = 0.693145751953125f;
     const float LN2_LO = 1.42860682030941723e-6f;
@@ -84,6 +85,7 @@ LUMEN_HD float lumen_expf_reduced(float x, int* ki_out) {
     p = fmaf(p, r, 1.0f);
     p = fmaf(p, r, 1.0f);
     *ki_out = ki;
+    *tbits_out = (uint32_t)lumen_float_bits(t);
     return p;
 }
 
@@ -92,8 +94,11 @@ LUMEN_HD float lumen_expf_reduced(float x, int* ki_out) {
  * lie in [-4.5, 0]). */
 LUMEN_HD float lumen_expf_core(float x) {
     int ki;
-    const float p = lumen_expf_reduced(x, &ki);
-    return p * lumen_pow2i(ki);
+    uint32_t tb;
+    const float p = lumen_expf_reduced(x, &ki, &tb);
+    /* 2^ki = bits (ki + 127) << 23 = (tb << 23) + (127 << 23) mod 2^32, as
+     * 0x4B400000 << 23 vanishes mod 2^32: one integer multiply-add */
+    return p * lumen_bits_to_float(tb * 8388608u + 0x3F800000u);
 }
 
 LUMEN_HD float lumen_expf(float x) {
@@ -101,7 +106,8 @@ LUMEN_HD float lumen_expf(float x) {
     if (x > 88.72283935546875f) return INFINITY;
     if (x < -103.97208404541015625f) return 0.0f;
     int ki;
-    const float p = lumen_expf_reduced(x, &ki);
+    uint32_t tb;
+    const float p = lumen_expf_reduced(x, &ki, &tb);
     if (ki > 127) return (p * lumen_pow2i(ki - 1)) * 2.0f;
     if (ki < -126) return (p * lumen_pow2i(ki + 64)) * lumen_pow2i(-64);
     return p * lumen_pow2i(ki);

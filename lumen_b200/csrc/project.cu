@@ -7,7 +7,7 @@
  * indices in Gaussian order (pipeline.mojo:141-149) and each appends one
  * key per covered tile (:152-157); the keys are then stably sorted (:166).
  *
- * K1: a block of 256 threads projects 256 consecutive Gaussians (their SH
+ * K1: a block of 128 threads projects 128 consecutive Gaussians (their SH
  * coefficients staged in shared memory by asynchronous copies) and scans
  * their visibility flags; the global offset comes from a decoupled look-back
  * over blocks taken in ticket order, so visible indices are exactly the
@@ -64,7 +64,8 @@ __device__ unsigned long long lookback64(const unsigned long long* desc, int blk
     return excl;
 }
 
-/* Block-wide exclusive scan of one value per thread (256 threads). */
+/* Block-wide exclusive scan of one value per thread (kThreads threads). */
+template <int kThreads>
 __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int x, unsigned int* warp_tot,
                                                              unsigned int* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -78,7 +79,7 @@ __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int x, uns
     __syncthreads();
     unsigned int before = 0, all = 0;
 #pragma unroll
-    for (int w = 0; w < kProjThreads / 32; ++w) {
+    for (int w = 0; w < kThreads / 32; ++w) {
         const unsigned int t = warp_tot[w];
         if (w < warp) before += t;
         all += t;
@@ -99,10 +100,10 @@ struct ProjSmem {
 constexpr int kViewWords = (int)(sizeof(ViewDesc) / 4);
 static_assert(sizeof(ViewDesc) % 4 == 0 && kViewWords <= kProjThreads - 32, "view copy layout");
 
-/* Each CTA takes a 256-Gaussian block by ticket (kPersistent: blocks until
+/* Each CTA takes a 128-Gaussian block by ticket (kPersistent: blocks until
  * the batch's blocks are exhausted, for a grid fixed in advance). Block b
  * belongs to the last view whose block_begin <= b, and covers that view's
- * Gaussians (b - block_begin) * 256 onward; visible indices run over the
+ * Gaussians (b - block_begin) * 128 onward; visible indices run over the
  * whole batch in block order. n_views_hint: the batch's view count, or 0
  * to read it from the table; with one view, the view is copied to shared
  * memory while the ticket is being taken. */
@@ -174,7 +175,7 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
             if (f.radii) f.radii[slot] = p.visible ? p.radius : 0;
         }
         unsigned int block_vis = 0;
-        const unsigned int vis_local = block_exclusive_scan(p.visible ? 1u : 0u, s.warp_tot, &block_vis);
+        const unsigned int vis_local = block_exclusive_scan<kProjThreads>(p.visible ? 1u : 0u, s.warp_tot, &block_vis);
         if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_vis);
         if (warp == 0) {
             const unsigned long long e = blk > 0 ? lookback64(lb, blk, &ctrl->error_flags) : 0ull;
@@ -227,21 +228,21 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
 
 struct EmitSmem {
     unsigned int blk;
-    unsigned int warp_tot[kProjThreads / 32];
+    unsigned int warp_tot[kEmitThreads / 32];
     unsigned long long inst_base;
-    unsigned int incl[kProjThreads];
-    unsigned int vis[kProjThreads];
-    unsigned int rect_lo[kProjThreads];   /* min_tx | min_ty << 16 */
-    unsigned int width[kProjThreads];     /* tiles per rectangle row */
-    unsigned int tile_base[kProjThreads]; /* batch-wide id of the view's tile 0 */
-    unsigned int tiles_x[kProjThreads];
+    unsigned int incl[kEmitThreads];
+    unsigned int vis[kEmitThreads];
+    unsigned int rect_lo[kEmitThreads];   /* min_tx | min_ty << 16 */
+    unsigned int width[kEmitThreads];     /* tiles per rectangle row */
+    unsigned int tile_base[kEmitThreads]; /* batch-wide id of the view's tile 0 */
+    unsigned int tiles_x[kEmitThreads];
     unsigned long long key_or, key_or_not;
 };
 
 /* Like project_kernel: 256 consecutive splats of the depth order per ticket.
  * Tile ids are batch-wide (view tile_begin + ty * tiles_x + tx). */
 template <bool kPersistent>
-__global__ void __launch_bounds__(kProjThreads)
+__global__ void __launch_bounds__(kEmitThreads)
 emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, unsigned long long* lb) {
     __shared__ EmitSmem s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -256,8 +257,8 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         }
         __syncthreads();
         const int blk = (int)s.blk;
-        if ((long long)blk * kProjThreads >= V) break;   /* past the visible splats: no look-back waits on it */
-        const long long p = (long long)blk * kProjThreads + tid;
+        if ((long long)blk * kEmitThreads >= V) break;   /* past the visible splats: no look-back waits on it */
+        const long long p = (long long)blk * kEmitThreads + tid;
         unsigned int cnt = 0, v = 0;
         if (p < V) {
             v = order[p];
@@ -273,7 +274,7 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
             s.tiles_x[tid] = (unsigned int)vd.tiles_x;
         }
         unsigned int block_inst = 0;
-        const unsigned int excl = block_exclusive_scan(cnt, s.warp_tot, &block_inst);
+        const unsigned int excl = block_exclusive_scan<kEmitThreads>(cnt, s.warp_tot, &block_inst);
         if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_inst);
         s.incl[tid] = excl + cnt;
         s.vis[tid] = v;
@@ -287,8 +288,8 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         __syncthreads();
         const unsigned long long inst_base = s.inst_base;
         unsigned long long kor = 0ull, knot = 0ull;
-        for (unsigned int j = tid; j < block_inst; j += kProjThreads) {
-            int lo = 0, hi = kProjThreads - 1;
+        for (unsigned int j = tid; j < block_inst; j += kEmitThreads) {
+            int lo = 0, hi = kEmitThreads - 1;
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
                 if (s.incl[mid] > j) hi = mid; else lo = mid + 1;
@@ -323,7 +324,7 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
                 atomicOr(&ctrl->tile_sort.key_or, s.key_or);
                 atomicOr(&ctrl->tile_sort.key_or_not, s.key_or_not);
             }
-            if ((long long)blk == (V - 1) / kProjThreads) {
+            if ((long long)blk == (V - 1) / kEmitThreads) {
                 const unsigned long long K = inst_base + block_inst;
                 ctrl->n_instances = K;
                 ctrl->tile_sort.n = K;
@@ -351,7 +352,7 @@ void prime_persistent_launches() {
     cudaFuncSetAttribute(project_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kProjStageBytes);
     cudaFuncSetAttribute(project_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kProjStageBytes);
     g_project_per_sm = resident_ctas((const void*)project_kernel<true>, kProjThreads, kProjStageBytes);
-    g_emit_per_sm = resident_ctas((const void*)emit_kernel<true>, kProjThreads, 0);
+    g_emit_per_sm = resident_ctas((const void*)emit_kernel<true>, kEmitThreads, 0);
 }
 
 /* Plain launches: one CTA per block (n_blocks known on the host).
@@ -374,9 +375,10 @@ void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, uns
     if (n_blocks <= 0) return;
     if (persistent) {
         const int per_sm = g_emit_per_sm > 0 ? g_emit_per_sm : 1;
-        emit_kernel<true><<<per_sm * num_sms, kProjThreads, 0, st>>>(vt, f, ctrl, lb);
+        emit_kernel<true><<<per_sm * num_sms, kEmitThreads, 0, st>>>(vt, f, ctrl, lb);
     } else {
-        emit_kernel<false><<<(unsigned int)n_blocks, kProjThreads, 0, st>>>(vt, f, ctrl, lb);
+        emit_kernel<false><<<(unsigned int)((n_blocks * kProjThreads + kEmitThreads - 1) / kEmitThreads),
+                              kEmitThreads, 0, st>>>(vt, f, ctrl, lb);
     }
 }
 

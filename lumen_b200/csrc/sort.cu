@@ -424,8 +424,13 @@ void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long*
 }
 
 void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st) {
-    tile_ranges_kernel<<<num_sms * 4, 256, 0, st>>>(f.keys[0], f.keys[1], (long long)f.instance_capacity, vt,
-                                                    f.ranges, ctrl);
+    /* about one group of 4 keys per thread at full capacity (the loads are
+     * independent, so more threads in flight hide their latency) */
+    long long grid = ((long long)f.instance_capacity + 1023) / 1024;
+    if (grid < num_sms * 4) grid = num_sms * 4;
+    if (grid > (1ll << 20)) grid = 1ll << 20;
+    tile_ranges_kernel<<<(unsigned int)grid, 256, 0, st>>>(f.keys[0], f.keys[1], (long long)f.instance_capacity, vt,
+                                                           f.ranges, ctrl);
 }
 
 void launch_key_stats64(const unsigned long long* keys, long long n, SortControl* sc, int num_sms, cudaStream_t st) {

@@ -53,7 +53,8 @@ struct Control {
     SortControl tile_sort;               /* instances by tile id */
 };
 
-constexpr int kProjThreads = 256;
+constexpr int kProjThreads = 128;   /* Gaussians per projection block (a view's slots are a multiple) */
+constexpr int kEmitThreads = 256;   /* splats per emission block */
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;   /* 4096 keys per tile */
@@ -86,9 +87,9 @@ struct DevCamera {
 
 /* One view of a batch as the kernels read it. A batch is a list of views,
  * each with its own scene, camera and output image; a single-view frame is a
- * batch of one. Projection treats the batch as consecutive 256-Gaussian
+ * batch of one. Projection treats the batch as consecutive 128-Gaussian
  * blocks (block_begin: the view's first block; its Gaussian i has slot
- * block_begin * 256 + i), and tiles get batch-wide ids (tile_begin: the
+ * block_begin * 128 + i), and tiles get batch-wide ids (tile_begin: the
  * global id of the view's tile 0), so one sort orders every view at once:
  * the tile-id key carries the view in its high part. */
 struct ViewDesc {
@@ -126,7 +127,8 @@ __host__ __device__ constexpr inline size_t view_table_bytes(int max_views) {
  * 2048-key tiles x 256 x u32][tile-sort look-back: 8 passes x 4096-key tiles
  * x 256 x u32, which is also 4 passes x 2048-key tiles (8 passes for the
  * standalone 64-bit pair sort)]. n counts projection slots (the Gaussians
- * of all views, each view rounded up to 256). */
+ * of all views, each view rounded up to a multiple of kProjThreads). The
+ * emit look-back uses at most as many entries as the project look-back. */
 struct ScratchLayout {
     size_t control_off, proj_lb_off, emit_lb_off, table_off, depth_lb_off, tile_lb_off, total;
     int64_t proj_blocks, depth_tiles, sort_tiles;
