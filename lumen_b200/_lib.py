@@ -137,6 +137,14 @@ class LumenServeStats(C.Structure):
                 ("max_tiles", C.c_int64), ("max_instances", C.c_int64), ("max_pixels", C.c_int64)]
 
 
+# ---- lumen_ply.h --------------------------------------------------------------
+class LumenPlyInfo(C.Structure):
+    _fields_ = [("count", C.c_int64), ("binary", C.c_int32), ("sh_degree", C.c_int32), ("log_values", C.c_int32),
+                ("vertex_stride", C.c_int32), ("data_offset", C.c_int64)]
+
+
+PLY_VALUES_AUTO, PLY_VALUES_LINEAR, PLY_VALUES_LOG = 0, 1, 2
+
 SPLAT_RECORD_BYTES = 48
 
 # name -> (restype, argtypes); every symbol the two headers declare
@@ -204,6 +212,12 @@ SIGNATURES = {
                                          C.POINTER(LumenGpuFrame), _P]),
     "lumen_gpu_render_batch_timed": (C.c_int, [C.POINTER(LumenGpuBatchView), C.c_int32,
                                                C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame), _P, _P]),
+    # lumen_ply.h
+    "lumen_ply_info": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(LumenPlyInfo)]),
+    "lumen_ply_load_host": (C.c_int, [C.c_char_p, C.c_int32, _P, _P, _P, _P, _P, C.c_int64,
+                                      C.POINTER(LumenPlyInfo)]),
+    "lumen_ply_load_device": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(LumenGpuGaussians),
+                                        C.POINTER(LumenPlyInfo), _P]),
     # lumen_serve.h
     "lumen_server_default_config": (LumenServerConfig, []),
     "lumen_server_create": (_P, [C.POINTER(LumenServerConfig)]),

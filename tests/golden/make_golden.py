@@ -1,5 +1,10 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
+sdk_cloud.ply + sdk_cloud_expected.npz: a 7-splat cloud written by the
+reference Python SDK's GaussianCloud.save_ply (python/lumen/cloud.py:131-161)
+and the values its load_ply (:163-199) reads back (columns x y z scale rot
+opacity f_dc, "%.6f"), for the PLY reader's test.
+
 capi_synthetic.npz: the splats the reference C library
 (c_api/src/lumen_c.c:156-256, built into oracle/_ref/liblumen_ref.so by
 ``make -C oracle ref``) generates for lumen_create_synthetic_cube(4, 2.0) and
@@ -46,5 +51,33 @@ def main():
                         **{"sphere_128_1.5": dump(lib.lumen_create_synthetic_sphere(128, 1.5))})
 
 
+def sdk_ply():
+    """Needs the reference source tree (its Python SDK) on this machine."""
+    import sys
+    sys.path.insert(0, "/root/reference/python")
+    from lumen.cloud import Gaussian3D, GaussianCloud
+    rng = np.random.default_rng(7)
+    cloud = GaussianCloud()
+    for _ in range(7):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        sh = [0.0] * 48
+        sh[:3] = [float(v) for v in rng.normal(0.5, 0.2, 3)]
+        cloud.add(Gaussian3D(position=tuple(float(v) for v in rng.uniform(-2, 2, 3)),
+                             scale=tuple(float(v) for v in rng.uniform(0.01, 0.3, 3)),
+                             rotation=tuple(float(v) for v in q), opacity=float(rng.uniform(0.05, 1.0)),
+                             sh_coeffs=sh))
+    path = os.path.join(HERE, "sdk_cloud.ply")
+    cloud.save_ply(path)
+    back = GaussianCloud.load_ply(path)
+    np.savez_compressed(os.path.join(HERE, "sdk_cloud_expected.npz"),
+                        means=np.array([g.position for g in back.splats], np.float32),
+                        scales=np.array([g.scale for g in back.splats], np.float32),
+                        quats=np.array([g.rotation for g in back.splats], np.float32),
+                        opacities=np.array([g.opacity for g in back.splats], np.float32),
+                        sh=np.array([g.sh_coeffs for g in back.splats], np.float32))
+
+
 if __name__ == "__main__":
     main()
+    sdk_ply()
