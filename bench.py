@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-fwd-bwd", action="store_true")
     p.add_argument("--no-multiview", action="store_true")
     p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--no-train", action="store_true")
+    p.add_argument("--no-depth", action="store_true")
+    p.add_argument("--no-picking", action="store_true")
     p.add_argument("--serve-requests", type=int, default=1000)
     return p.parse_args()
 
@@ -396,6 +399,173 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
             "autograd_api_steps_per_s": 1000.0 / api_ms, "visible": V, "instances": K,
             "roofline": {"bytes": total, "achieved": total / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                          "frac": total / (ms * 1e-3) / 1e9 / hbm_peak}}
+
+
+def train_leg(dev, steps):
+    """The training step around the adjoint (lumen_b200.train.Trainer, the
+    reference's TrainingCoordinator.train_step with real gradients) on the
+    500k-Gaussian 1080p scene: forward, L1 + PSNR, backward, Adam on
+    positions and opacity, view-space accumulation, metrics read back each
+    step (as the reference returns them). Then one density-control pass over
+    the accumulated gradients, timed on the device."""
+    import numpy as np
+    import torch
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    from lumen_b200 import train as T
+    from lumen_b200.types import RenderOptions
+    n = 500_000
+    sc = scenes.box_scene(n, seed=3)
+    s, op = sc.activated()
+    tg = scenes.perturbed(sc, seed=33)
+    ts, top = tg.activated()
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    opt = RenderOptions(term_mode=1)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    target = R.render(t(tg.means), t(ts), t(tg.quats), t(top).reshape(-1), t(tg.sh).reshape(n, 48), cam, opt).rgb
+    cfg = T.default_config()
+    cfg.densify_from_iter = 10 ** 9          # density control timed separately below
+    tr = T.Trainer(sc.means, s, sc.quats, op, sc.sh.reshape(n, 48), config=cfg, options=opt, scene_extent=6.0,
+                   device=dev)
+    for it in range(1, 4):
+        tr.train_step(cam, target, it)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    losses = []
+    for it in range(4, 4 + steps):
+        losses.append(tr.train_step(cam, target, it).loss)
+    torch.cuda.synchronize(dev)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    d0 = time.perf_counter()
+    cl, sp, pr = tr.densify_and_prune()
+    torch.cuda.synchronize(dev)
+    densify_wall_ms = (time.perf_counter() - d0) * 1e3
+    return {"workload": "500k Gaussians, 1920x1080, linear parameters, L1 to a perturbed copy of the scene",
+            "steps_per_s": 1000.0 / ms, "ms_per_step": ms, "loss_first": losses[0], "loss_last": losses[-1],
+            "timing": "host wall clock per step (each step reads its loss and PSNR back)",
+            "densify": {"device_ms": tr.last_densify_ms, "wall_ms_with_allocation": densify_wall_ms,
+                        "cloned": cl, "split": sp, "pruned": pr, "count": tr.count,
+                        "observations": 3 + steps}}
+
+
+def depth_leg(dev, steps, warmup, hbm_peak):
+    """Depth products (lumen_gpu_depth_products: range, normals and the SDK
+    heatmap in one pass) on 1920x1080 depth buffers rendered from the 1M
+    scene. 16 buffers are cycled so inputs and outputs (0.6 GB) exceed L2.
+    Algorithmic bytes: 4 read + 12 (normal) + 3 (heatmap) written per pixel.
+    Also the oracle's time for the same products of one buffer on one host
+    thread."""
+    import numpy as np
+    import torch
+    from lumen_b200 import depth as D
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    from lumen_b200.types import RenderOptions
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sc = scenes.box_scene(1_000_000, seed=1)
+    s, op = sc.activated()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    d0 = R.render(t(sc.means), t(s), t(sc.quats), t(op).reshape(-1), t(sc.sh).reshape(-1, 48), cam,
+                  RenderOptions(compute_depth=True)).depth.contiguous()
+    nbuf = 16
+    depths = [d0 * (1.0 + 0.01 * i) for i in range(nbuf)]
+    outs = [D.products(d, normals=True, range=True, heatmap=True, near_plane=2.0, far_plane=14.0)
+            for d in depths]
+    from lumen_b200 import _lib as lib
+    structs = []
+    for o in outs:
+        st = lib.LumenDepthProducts()
+        st.normals, st.range, st.heatmap = o.normals.data_ptr(), o.range.data_ptr(), o.heatmap.data_ptr()
+        st.near_plane, st.far_plane = 2.0, 14.0
+        structs.append(st)
+    cdll = lib.load()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def launch(i):
+        lib.check(cdll.lumen_gpu_depth_products(depths[i % nbuf].data_ptr(), WIDTH, HEIGHT, C.byref(structs[i % nbuf]),
+                                             stream), "depth_products")
+
+    for i in range(max(warmup, 3)):
+        launch(i)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        launch(i)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    P = WIDTH * HEIGHT
+    alg = 19 * P
+    h = d0.cpu().numpy()
+    c0 = time.perf_counter()
+    O.depth_normals(h)
+    O.depth_min_max(h)
+    O.depth_heatmap(h, 2.0, 14.0)
+    cpu_ms = (time.perf_counter() - c0) * 1e3
+    return {"workload": "depth products of a 1920x1080 depth buffer (1M-Gaussian render): range, normals, heatmap",
+            "ms": ms, "buffers_per_s": 1000.0 / ms, "gpu_launches_per_buffer": 2,
+            "roofline": {"bound": "hbm", "bytes": alg, "achieved": alg / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / hbm_peak},
+            "l2": "16 buffers cycled, 0.6 GB of inputs and outputs",
+            "cpu_oracle_ms_one_thread": cpu_ms}
+
+
+def picking_leg(dev, steps, warmup):
+    """Picking on the 1M-Gaussian config-1 scene: the LBVH build (Morton
+    codes, radix sort, leaves and parents; synchronous) and closest-splat
+    casts for a 256x256 block of pixel positions under the config-1 camera.
+    Also the oracle's build and casts on one host thread for comparison."""
+    import numpy as np
+    import torch
+    from lumen_b200 import scenes
+    from lumen_b200 import spatial as S
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sc = scenes.box_scene(1_000_000, seed=1)
+    s, _ = sc.activated()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    means, scales = t(sc.means), t(s)
+    cam = scenes.camera_config1(WIDTH, HEIGHT)
+    for _ in range(2):
+        bvh = S.LBVH(means, scales)
+    torch.cuda.synchronize(dev)
+    b0 = time.perf_counter()
+    nb = max(3, min(steps, 10))
+    for _ in range(nb):
+        bvh = S.LBVH(means, scales)
+    torch.cuda.synchronize(dev)
+    build_ms = (time.perf_counter() - b0) * 1e3 / nb
+    ys, xs = np.mgrid[412:668, 832:1088]
+    px = t(np.stack([xs.reshape(-1) + 0.5, ys.reshape(-1) + 0.5], axis=1))
+    for _ in range(max(warmup, 3)):
+        raw = bvh.pick(cam, px)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        raw = bvh.pick(cam, px)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    pick_ms = e0.elapsed_time(e1) / steps
+    hits = int((raw[:, 0] != 0).sum().item())
+    c0 = time.perf_counter()
+    nodes, idx, root, _ = O.bvh_build(sc.means, s)
+    cpu_build_ms = (time.perf_counter() - c0) * 1e3
+    sample = np.asarray(px.cpu().numpy())[::256]
+    c1 = time.perf_counter()
+    for x, y in sample:
+        o, d = O.generate_ray(cam, x, y)
+        O.raycast(nodes, idx, root, sc.means, s, o, d)
+    cpu_ray_us = (time.perf_counter() - c1) * 1e6 / sample.shape[0]
+    n_rays = int(px.shape[0])
+    return {"workload": "LBVH over 1M Gaussians; picks at a 256x256 pixel block, 1920x1080 camera",
+            "build_ms": build_ms, "pick_ms": pick_ms, "rays_per_s": n_rays / (pick_ms * 1e-3), "rays": n_rays,
+            "hits": hits, "build_timing": "host wall clock per synchronous build",
+            "cpu_oracle_one_thread": {"build_ms": cpu_build_ms, "us_per_ray": cpu_ray_us,
+                                      "sample": f"{sample.shape[0]} of the rays"}}
 
 
 def multiview_leg(dev, steps, warmup, hbm_peak):
@@ -744,6 +914,12 @@ def main():
         line["serving"] = serving_leg(dev, args.serve_requests, 24 << 30)
     if not args.no_fwd_bwd:
         line["fwd_bwd"] = fwd_bwd_leg(dev, min(steps, 100), args.warmup, hbm_peak)
+    if not args.no_train:
+        line["train_step"] = train_leg(dev, min(steps, 50))
+    if not args.no_depth:
+        line["depth_products"] = depth_leg(dev, min(steps, 200), args.warmup, hbm_peak)
+    if not args.no_picking:
+        line["picking"] = picking_leg(dev, min(steps, 50), args.warmup)
     if not args.no_e2e:
         e2e = e2e_rasterize(sc, scales, opac, steps, args.warmup)
         if pg:   # replicas: the slowest rank's rate times the number of ranks

@@ -145,6 +145,46 @@ class LumenPlyInfo(C.Structure):
 
 PLY_VALUES_AUTO, PLY_VALUES_LINEAR, PLY_VALUES_LOG = 0, 1, 2
 
+
+class LumenTrainingConfig(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("position_lr_init", C.c_float), ("position_lr_final", C.c_float),
+                ("feature_lr", C.c_float), ("opacity_lr", C.c_float), ("scaling_lr", C.c_float),
+                ("rotation_lr", C.c_float), ("lambda_dssim", C.c_float), ("densify_from_iter", C.c_int32),
+                ("densify_until_iter", C.c_int32), ("densification_interval", C.c_int32),
+                ("opacity_reset_interval", C.c_int32), ("densify_grad_threshold", C.c_float),
+                ("prune_opacity_threshold", C.c_float), ("max_screen_size_ratio", C.c_float)]
+
+
+class LumenAdamState(C.Structure):
+    _fields_ = [("m_pos", _P), ("v_pos", _P), ("m_opacity", _P), ("v_opacity", _P), ("step", C.c_int64)]
+
+
+class LumenDepthProducts(C.Structure):
+    _fields_ = [("normals", _P), ("range", _P), ("heatmap", _P), ("near_plane", C.c_double),
+                ("far_plane", C.c_double)]
+
+
+class LumenBvhNode(C.Structure):
+    _fields_ = [("min_pt", C.c_float * 3), ("left_child", C.c_int32), ("max_pt", C.c_float * 3),
+                ("right_child", C.c_int32)]
+
+
+class LumenGpuBvh(C.Structure):
+    _fields_ = [("nodes", _P), ("splat_index", _P), ("leaf_count", C.c_int64), ("node_count", C.c_int64),
+                ("root_index", C.c_int64)]
+
+
+class LumenRay(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("direction", C.c_float * 3)]
+
+
+class LumenRayHit(C.Structure):
+    _fields_ = [("hit", C.c_int32), ("splat_index", C.c_int32), ("distance", C.c_float), ("point", C.c_float * 3)]
+
+
+class LumenDensifyStats(C.Structure):
+    _fields_ = [("cloned", C.c_int64), ("split", C.c_int64), ("pruned", C.c_int64), ("count", C.c_int64)]
+
 SPLAT_RECORD_BYTES = 48
 
 # name -> (restype, argtypes); every symbol the two headers declare
@@ -229,6 +269,30 @@ SIGNATURES = {
     "lumen_serve_admit": (C.c_int32, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64), C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                       C.c_int64, C.c_int64]),
+    # lumen_train.h
+    "lumen_training_default_config": (LumenTrainingConfig, []),
+    "lumen_training_should_densify": (C.c_int32, [C.POINTER(LumenTrainingConfig), C.c_int64]),
+    "lumen_training_should_reset_opacity": (C.c_int32, [C.POINTER(LumenTrainingConfig), C.c_int64]),
+    "lumen_gpu_adam_step": (C.c_int, [C.POINTER(LumenGpuGaussians), _P, _P, C.POINTER(LumenAdamState),
+                                      C.POINTER(LumenTrainingConfig), _P]),
+    "lumen_gpu_accumulate_viewspace": (C.c_int, [_P, C.c_int32, _P, C.c_int64, C.c_float, C.c_float, _P, _P, _P]),
+    "lumen_gpu_densify_scratch_bytes": (C.c_size_t, [C.c_int64]),
+    "lumen_gpu_densify_and_prune": (C.c_int, [C.POINTER(LumenGpuGaussians), _P, _P, C.POINTER(LumenTrainingConfig),
+                                              C.c_float, C.POINTER(LumenGpuGaussians), C.POINTER(LumenAdamState),
+                                              C.POINTER(LumenAdamState), _P, C.c_size_t,
+                                              C.POINTER(LumenDensifyStats), _P]),
+    "lumen_gpu_reset_opacities": (C.c_int, [_P, C.c_int64, C.c_float, _P]),
+    "lumen_gpu_psnr": (C.c_int, [_P, _P, C.c_int64, _P, _P, _P]),
+    # lumen_depth.h
+    "lumen_gpu_depth_products": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(LumenDepthProducts), _P]),
+    # lumen_spatial.h
+    "lumen_bvh_node_count": (C.c_int64, [C.c_int64]),
+    "lumen_gpu_bvh_scratch_bytes": (C.c_size_t, [C.c_int64]),
+    "lumen_gpu_bvh_build": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenGpuBvh), _P, C.c_size_t, _P]),
+    "lumen_gpu_raycast": (C.c_int, [C.POINTER(LumenGpuBvh), C.POINTER(LumenGpuGaussians), _P, C.c_int64, C.c_float,
+                                    _P, _P]),
+    "lumen_gpu_pick_pixels": (C.c_int, [C.POINTER(LumenGpuBvh), C.POINTER(LumenGpuGaussians),
+                                        C.POINTER(LumenViewCamera), _P, C.c_int64, C.c_float, _P, _P, _P]),
     "lumen_gpu_stage_timer_read": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int)]),
 }
 

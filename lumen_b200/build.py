@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblumen.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["project.cu", "sort.cu", "composite.cu", "backward.cu", "forward.cu", "capi.cu", "noalloc.cu", "serve.cu", "ply.cu"]
+SOURCES = ["project.cu", "sort.cu", "composite.cu", "backward.cu", "forward.cu", "capi.cu", "noalloc.cu", "serve.cu", "ply.cu", "train.cu", "depth.cu", "spatial.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

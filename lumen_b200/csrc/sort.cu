@@ -437,6 +437,10 @@ void launch_key_stats64(const unsigned long long* keys, long long n, SortControl
     key_stats_kernel<unsigned long long><<<num_sms * 2, 256, 0, st>>>(keys, n, sc);
 }
 
+void launch_key_stats32(const unsigned int* keys, long long n, SortControl* sc, int num_sms, cudaStream_t st) {
+    key_stats_kernel<unsigned int><<<num_sms * 2, 256, 0, st>>>(keys, n, sc);
+}
+
 void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_mode, unsigned long long* out,
                           int num_sms, cudaStream_t st) {
     sorted_keys64_kernel<<<num_sms * 4, 256, 0, st>>>(f.keys[0], f.keys[1], f.vals[0], f.vals[1], f.records,

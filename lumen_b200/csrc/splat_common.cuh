@@ -480,4 +480,62 @@ __device__ __forceinline__ void st_volatile_u32(unsigned int* p, unsigned int v)
     *reinterpret_cast<volatile unsigned int*>(p) = v;
 }
 
+/* Warp-parallel decoupled look-back over 64-bit descriptors: the sum of all
+ * blocks before `blk`. Called by one full warp. */
+__device__ __forceinline__ unsigned long long lookback64(const unsigned long long* desc, int blk, unsigned int* err) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long excl = 0;
+    int base = blk - 1;
+    while (base >= 0) {
+        int idx = base - lane;
+        unsigned long long v = kDescIncl64;   /* before block 0: inclusive 0 */
+        if (idx >= 0) {
+            int spins = 0;
+            for (;;) {
+                v = ld_volatile_u64(desc + idx);
+                if (v >> 62) break;
+                if (++spins >= kSpinLimit) {
+                    atomicOr(err, LUMEN_GPU_ERR_SPIN_TIMEOUT);
+                    v = kDescIncl64;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        unsigned int incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+        int first = incl ? __ffs(incl) - 1 : 31;
+        unsigned long long c = lane <= first ? (v & kDescMask64) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        excl += c;
+        if (incl) break;
+        base -= 32;
+    }
+    return excl;
+}
+
+/* Block-wide exclusive scan of one value per thread (kThreads threads). */
+template <int kThreads>
+__device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int x, unsigned int* warp_tot,
+                                                             unsigned int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    unsigned int before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        const unsigned int t = warp_tot[w];
+        if (w < warp) before += t;
+        all += t;
+    }
+    *total = all;
+    return before + incl - x;
+}
+
 }  // namespace lumen

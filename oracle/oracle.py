@@ -3,8 +3,11 @@
 Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s cpu_baseline leg and
 reference arm import this module, as the checker and the timed CPU baseline.
 The oracle restates the reference's Mojo forward path
-(src/raster/pipeline.mojo:48-231); see lumen_oracle.cpp for the per-function
-citations. Parity pinning: the reference's own known-answer tests, restated in
+(src/raster/pipeline.mojo:48-231), its training-step pieces (optimizer,
+density control, PSNR, view-space accumulation), the depth-buffer
+products and picking (Morton codes, LBVH, ray casts); see lumen_oracle.cpp and
+train_oracle.cpp, depth_oracle.cpp and spatial_oracle.cpp for the
+per-function citations. Parity pinning: the reference's own known-answer tests, restated in
 tests/test_oracle_kat.py.
 """
 from __future__ import annotations
@@ -76,6 +79,29 @@ def lib():
         _lib.oracle_encode_key.argtypes = [C.c_uint32, C.c_float, C.c_int]
         _lib.oracle_l1_loss.restype = C.c_float
         _lib.oracle_l1_loss.argtypes = [_P, _P, C.c_int64, _P]
+        _lib.oracle_position_lr.restype = C.c_float
+        _lib.oracle_position_lr.argtypes = [C.c_float, C.c_float, C.c_int32, C.c_int64]
+        _lib.oracle_adam_scalars.argtypes = [C.c_float, C.c_float, C.c_int64, _P, _P]
+        _lib.oracle_adam_step.argtypes = [_P] * 8 + [C.c_int64] + [C.c_float] * 7
+        _lib.oracle_densify_and_prune.restype = C.c_int64
+        _lib.oracle_densify_and_prune.argtypes = ([_P] * 7 + [C.c_int64, C.c_float, C.c_float, C.c_float] +
+                                                  [_P] * 13 + [_P, _P, _P])
+        _lib.oracle_reset_opacities.argtypes = [_P, C.c_int64, C.c_float]
+        _lib.oracle_psnr.restype = C.c_float
+        _lib.oracle_psnr.argtypes = [_P, _P, C.c_int64]
+        _lib.oracle_accumulate_viewspace.argtypes = [_P, C.c_int32, _P, C.c_int64, C.c_float, C.c_float, _P, _P]
+        _lib.oracle_depth_min_max.argtypes = [_P, C.c_int64, _P, _P]
+        _lib.oracle_depth_normal.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]
+        _lib.oracle_depth_normals.argtypes = [_P, C.c_int32, C.c_int32, _P]
+        _lib.oracle_depth_heatmap.argtypes = [_P, C.c_int64, C.c_double, C.c_double, _P]
+        _lib.oracle_expand_bits.restype = C.c_uint32
+        _lib.oracle_expand_bits.argtypes = [C.c_uint32]
+        _lib.oracle_morton3d.restype = C.c_uint32
+        _lib.oracle_morton3d.argtypes = [C.c_float] * 3
+        _lib.oracle_bvh_build.restype = C.c_int64
+        _lib.oracle_bvh_build.argtypes = [_P, _P, C.c_int64, _P, _P, _P]
+        _lib.oracle_raycast.argtypes = [_P, _P, C.c_int64, C.c_int64, _P, _P, C.c_int64, _P, _P, C.c_float, _P]
+        _lib.oracle_generate_ray.argtypes = [C.POINTER(OracleCamera), C.c_float, C.c_float, _P]
         for name, args in [("oracle_ewa_cov2d", [_P, _P, _P, C.c_float, C.c_float, C.c_float, _P]),
                            ("oracle_jacobian", [_P, C.c_float, C.c_float, _P]),
                            ("oracle_cov3d", [_P, _P, _P]),
@@ -233,3 +259,154 @@ def l1_loss(pred, target):
     g = np.zeros_like(p)
     loss = lib().oracle_l1_loss(_ptr(p), _ptr(t), p.shape[0], _ptr(g))
     return float(loss), g
+
+
+# ---------------------------------------------------------------- training step
+
+ADAM_BETA1, ADAM_BETA2, ADAM_EPS = np.float32(0.9), np.float32(0.999), np.float32(1e-8)
+
+
+def position_lr(init, final, iterations, iteration) -> float:
+    return float(lib().oracle_position_lr(float(init), float(final), int(iterations), int(iteration)))
+
+
+def adam_scalars(beta1, beta2, step):
+    a, b = np.zeros(1, np.float32), np.zeros(1, np.float32)
+    lib().oracle_adam_scalars(float(beta1), float(beta2), int(step), _ptr(a), _ptr(b))
+    return float(a[0]), float(b[0])
+
+
+def adam_step(means, opacities, grad_means, grad_op, m_pos, v_pos, m_op, v_op, pos_lr, opacity_lr, step):
+    """One AdamOptimizer.step in place on float32 arrays (means and moments
+    N x 3, opacities and their moments N); step is the counter after the
+    increment."""
+    for a in (means, opacities, m_pos, v_pos, m_op, v_op):
+        assert a.dtype == np.float32 and a.flags.c_contiguous
+    gm, go = _f32(grad_means), _f32(grad_op)
+    ib1, ib2 = adam_scalars(ADAM_BETA1, ADAM_BETA2, step)
+    lib().oracle_adam_step(_ptr(means), _ptr(opacities), _ptr(gm), _ptr(go), _ptr(m_pos), _ptr(v_pos), _ptr(m_op),
+                           _ptr(v_op), means.shape[0], float(pos_lr), float(opacity_lr), float(ADAM_BETA1),
+                           float(ADAM_BETA2), float(ADAM_EPS), ib1, ib2)
+
+
+def densify_and_prune(means, scales, quats, opacities, sh, vs_sum, vs_count, grad_thr, prune_thr, extent,
+                      moments=None):
+    """densify_and_prune on copies: returns (cloud dict, moments dict or None,
+    (cloned, split, pruned)). moments: dict m_pos, v_pos, m_op, v_op."""
+    f = lambda a, s: np.ascontiguousarray(a, np.float32).reshape(s)
+    n = int(np.asarray(means).shape[0])
+    src = [f(means, (n, 3)), f(scales, (n, 3)), f(quats, (n, 4)), f(opacities, (n,)), f(sh, (n, 48))]
+    vs, vc = f(vs_sum, (n,)), np.ascontiguousarray(vs_count, np.int32).reshape(n)
+    cap = 2 * max(n, 1)
+    out = [np.zeros((cap,) + a.shape[1:], np.float32) for a in src]
+    names = ("m_pos", "v_pos", "m_op", "v_op")
+    sm = [f(moments[k], (n, 3) if k.endswith("pos") else (n,)) for k in names] if moments else [None] * 4
+    dm = [np.zeros((cap,) + m.shape[1:], np.float32) for m in sm] if moments else [None] * 4
+    c, s, p = (np.zeros(1, np.int64) for _ in range(3))
+    k = lib().oracle_densify_and_prune(*[_ptr(a) for a in src], _ptr(vs), _ptr(vc), n, float(grad_thr),
+                                       float(prune_thr), float(extent), *[_ptr(a) for a in out],
+                                       *[_ptr(a) for a in sm], *[_ptr(a) for a in dm], _ptr(c), _ptr(s), _ptr(p))
+    cloud = {name: a[:k] for name, a in zip(("means", "scales", "quats", "opacities", "sh"), out)}
+    mom = {name: a[:k] for name, a in zip(names, dm)} if moments else None
+    return cloud, mom, (int(c[0]), int(s[0]), int(p[0]))
+
+
+def reset_opacities(op, max_value=0.01):
+    assert op.dtype == np.float32 and op.flags.c_contiguous
+    lib().oracle_reset_opacities(_ptr(op), op.shape[0], float(max_value))
+
+
+def psnr(pred, target) -> float:
+    p, t = _f32(pred).reshape(-1), _f32(target).reshape(-1)
+    return float(lib().oracle_psnr(_ptr(p), _ptr(t), p.shape[0]))
+
+
+def accumulate_viewspace(grad2d, stride, radii, vs_sum, vs_count, scale_x=1.0, scale_y=1.0):
+    """In place on vs_sum (float32) and vs_count (int32)."""
+    g = _f32(grad2d)
+    r = np.ascontiguousarray(radii, np.int32)
+    lib().oracle_accumulate_viewspace(_ptr(g), int(stride), _ptr(r), r.shape[0], float(scale_x), float(scale_y),
+                                      _ptr(vs_sum), _ptr(vs_count))
+
+
+# ---------------------------------------------------------------- depth products
+
+def depth_min_max(depth):
+    d = _f32(depth).reshape(-1)
+    lo, hi = np.zeros(1, np.float32), np.zeros(1, np.float32)
+    lib().oracle_depth_min_max(_ptr(d), d.shape[0], _ptr(lo), _ptr(hi))
+    return float(lo[0]), float(hi[0])
+
+
+def depth_normal(depth, x, y):
+    d = _f32(depth)
+    h, w = d.shape
+    out = np.zeros(3, np.float32)
+    lib().oracle_depth_normal(_ptr(d), w, h, x, y, _ptr(out))
+    return out
+
+
+def depth_normals(depth):
+    d = _f32(depth)
+    h, w = d.shape
+    out = np.zeros((h, w, 3), np.float32)
+    lib().oracle_depth_normals(_ptr(d), w, h, _ptr(out))
+    return out
+
+
+def depth_heatmap(depth, near_plane=0.5, far_plane=10.0):
+    d = _f32(depth)
+    out = np.zeros(d.shape + (3,), np.uint8)
+    lib().oracle_depth_heatmap(_ptr(d), d.size, float(near_plane), float(far_plane), _ptr(out))
+    return out
+
+
+# ---------------------------------------------------------------- picking
+
+BVH_NODE_DTYPE = np.dtype([("min_pt", "<f4", 3), ("left_child", "<i4"), ("max_pt", "<f4", 3),
+                           ("right_child", "<i4")])
+RAY_HIT_DTYPE = np.dtype([("hit", "<i4"), ("splat_index", "<i4"), ("distance", "<f4"), ("point", "<f4", 3)])
+
+
+def expand_bits(v: int) -> int:
+    return int(lib().oracle_expand_bits(int(v)))
+
+
+def morton3d(nx, ny, nz) -> int:
+    return int(lib().oracle_morton3d(float(nx), float(ny), float(nz)))
+
+
+def bvh_build(means, scales):
+    """LBVH.build_from_cloud: (nodes [BVH_NODE_DTYPE], splat_index [n] int32,
+    root index, Morton codes [n] uint32 in input order)."""
+    m, s = _f32(means).reshape(-1, 3), _f32(scales).reshape(-1, 3)
+    n = m.shape[0]
+    total, count = n, n
+    while count > 1:
+        count = (count + 1) // 2
+        total += count
+    nodes = np.zeros(max(total, 1), BVH_NODE_DTYPE)
+    idx = np.zeros(max(n, 1), np.int32)
+    codes = np.zeros(max(n, 1), np.uint32)
+    k = lib().oracle_bvh_build(_ptr(m), _ptr(s), n, nodes.ctypes.data, _ptr(idx), _ptr(codes))
+    return nodes[:k], idx[:n], k - 1 if k > 0 else -1, codes[:n]
+
+
+def raycast(nodes, splat_index, root, means, scales, origin, direction, max_dist=1000.0):
+    """raycast_closest_splat for one ray: a RAY_HIT_DTYPE record."""
+    m, s = _f32(means).reshape(-1, 3), _f32(scales).reshape(-1, 3)
+    nd = np.ascontiguousarray(nodes, BVH_NODE_DTYPE)
+    si = np.ascontiguousarray(splat_index, np.int32)
+    o, d = _f32(origin).reshape(3), _f32(direction).reshape(3)
+    out = np.zeros(1, RAY_HIT_DTYPE)
+    lib().oracle_raycast(nd.ctypes.data, _ptr(si), nd.shape[0], int(root), _ptr(m), _ptr(s), m.shape[0], _ptr(o),
+                         _ptr(d), float(max_dist), out.ctypes.data)
+    return out[0]
+
+
+def generate_ray(cam, px, py):
+    """PinholeCamera.generate_ray: (origin [3], unit direction [3])."""
+    oc = make_camera(cam)
+    out = np.zeros(6, np.float32)
+    lib().oracle_generate_ray(C.byref(oc), float(px), float(py), _ptr(out))
+    return out[:3], out[3:]

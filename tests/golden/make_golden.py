@@ -9,8 +9,17 @@ capi_synthetic.npz: the splats the reference C library
 (c_api/src/lumen_c.c:156-256, built into oracle/_ref/liblumen_ref.so by
 ``make -C oracle ref``) generates for lumen_create_synthetic_cube(4, 2.0) and
 lumen_create_synthetic_sphere(128, 1.5), as [n, 59] float32 rows in
-LumenGaussian field order. The reference source is needed only to run this
-script; the tests read the committed .npz.
+LumenGaussian field order.
+
+sdk_depth_heatmap.npz: a 12 x 16 depth buffer holding the edge cases of the
+SDK's depth visualisation (background at <= 0 and >= 999, the near and far
+planes, values beyond them, infinities, NaN) plus seeded depths, and the RGB
+bytes that the reference Python SDK's export_depth_visualization
+(python/lumen/visualizer.py:16-48) writes for it with its default planes and
+with near 1.25, far 7.5.
+
+The reference source is needed only to run this script; the tests read the
+committed files.
 """
 import ctypes as C
 import os
@@ -78,6 +87,37 @@ def sdk_ply():
                         sh=np.array([g.sh_coeffs for g in back.splats], np.float32))
 
 
+def sdk_depth_heatmap():
+    """Needs the reference source tree (its Python SDK) on this machine."""
+    import sys
+    import tempfile
+    sys.path.insert(0, "/root/reference/python")
+    from lumen.visualizer import export_depth_visualization
+    rng = np.random.default_rng(11)
+    h, w = 12, 16
+    d = rng.uniform(0.2, 12.0, h * w).astype(np.float32)
+    edge = [0.0, -1.0, -0.0, 1e-4, 0.001, 0.5, 10.0, 998.99, 999.0, 1e4, np.inf, -np.inf, np.nan,
+            0.4999, 10.0001, 5.25, 0.5 + 9.5 / 255.0, 3.0]
+    d[:len(edge)] = np.array(edge, np.float32)
+    d = d.reshape(h, w)
+    out = {"depth": d}
+    for tag, kw in (("default", {}), ("near1.25_far7.5", {"near_plane": 1.25, "far_plane": 7.5})):
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "d.ppm")
+            export_depth_visualization(path, w, h, [float(v) for v in d.reshape(-1)], **kw)
+            raw = open(path, "rb").read()
+        header = f"P6\n{w} {h}\n255\n".encode("ascii")
+        assert raw.startswith(header)
+        out[tag] = np.frombuffer(raw[len(header):], np.uint8).reshape(h, w, 3)
+    np.savez_compressed(os.path.join(HERE, "sdk_depth_heatmap.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
-    sdk_ply()
+    import sys
+    which = sys.argv[1:] or ["capi", "ply", "depth"]
+    if "capi" in which:
+        main()
+    if "ply" in which:
+        sdk_ply()
+    if "depth" in which:
+        sdk_depth_heatmap()

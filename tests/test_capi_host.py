@@ -17,7 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = []
-    for h in ("lumen.h", "lumen_gpu.h", "lumen_serve.h", "lumen_ply.h"):
+    for h in ("lumen.h", "lumen_gpu.h", "lumen_serve.h", "lumen_ply.h", "lumen_train.h", "lumen_depth.h", "lumen_spatial.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         names += re.findall(r"\b(lumen_\w+)\s*\(", src)
@@ -64,13 +64,15 @@ def test_struct_sizes():
 GPU_STRUCTS = ["LumenGpuGaussians", "LumenViewCamera", "LumenRenderOptions", "LumenSplatRecord", "LumenGpuFrame",
                "LumenGpuImage", "LumenGpuCounts", "LumenGpuGradients", "LumenGpuBatchView", "LumenGpuLaunch",
                "LumenServerConfig",
-               "LumenServeResult", "LumenServeStats", "LumenPlyInfo"]
+               "LumenServeResult", "LumenServeStats", "LumenPlyInfo", "LumenTrainingConfig", "LumenAdamState",
+               "LumenDensifyStats", "LumenDepthProducts", "LumenBvhNode", "LumenGpuBvh", "LumenRay",
+               "LumenRayHit"]
 
 
 def test_ctypes_layouts_match_the_header(tmp_path):
     """sizeof and every field offset of the ctypes mirrors equal what a C
     compiler gives for include/lumen_gpu.h and include/lumen_serve.h."""
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lumen_serve.h"', '#include "lumen_ply.h"',
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lumen_serve.h"', '#include "lumen_ply.h"', '#include "lumen_train.h"', '#include "lumen_depth.h"', '#include "lumen_spatial.h"',
              "int main(void) {"]
     for name in GPU_STRUCTS:
         if not hasattr(L, name):
