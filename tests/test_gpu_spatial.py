@@ -33,11 +33,16 @@ def _cloud(n, seed, flat=False, nan=False):
 
 
 def _nodes_equal(bvh, nodes, idx):
+    """Bit-equal nodes; a NaN box coordinate (from a NaN position) matches
+    any NaN, since device and host NaN payloads differ."""
     k = bvh.node_count()
     got = bvh.nodes[:k].cpu().numpy().view(np.uint32)
     want = np.ascontiguousarray(nodes).view(np.uint32).reshape(-1, 8)
     assert got.shape == want.shape
-    assert np.array_equal(got, want)
+    gf, wf = got.view(np.float32), want.view(np.float32)
+    nan_ok = np.isnan(gf) & np.isnan(wf)
+    nan_ok[:, [3, 7]] = False                          # child indices are integers
+    assert ((got == want) | nan_ok).all()
     assert np.array_equal(bvh.splat_index[:len(idx)].cpu().numpy(), idx)
 
 
