@@ -558,7 +558,7 @@ def picking_leg(dev, steps, warmup):
     c1 = time.perf_counter()
     for x, y in sample:
         o, d = O.generate_ray(cam, x, y)
-        O.raycast(nodes, idx, root, sc.means, s, o, d)
+        O.raycast(nodes, idx, root, sc.means, s, o, d, unit=True)
     cpu_ray_us = (time.perf_counter() - c1) * 1e6 / sample.shape[0]
     n_rays = int(px.shape[0])
     return {"workload": "LBVH over 1M Gaussians; picks at a 256x256 pixel block, 1920x1080 camera",

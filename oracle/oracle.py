@@ -102,6 +102,7 @@ def lib():
         _lib.oracle_bvh_build.argtypes = [_P, _P, C.c_int64, _P, _P, _P]
         _lib.oracle_raycast.argtypes = [_P, _P, C.c_int64, C.c_int64, _P, _P, C.c_int64, _P, _P, C.c_float, _P]
         _lib.oracle_generate_ray.argtypes = [C.POINTER(OracleCamera), C.c_float, C.c_float, _P]
+        _lib.oracle_ray_direction.argtypes = [_P, _P]
         for name, args in [("oracle_ewa_cov2d", [_P, _P, _P, C.c_float, C.c_float, C.c_float, _P]),
                            ("oracle_jacobian", [_P, C.c_float, C.c_float, _P]),
                            ("oracle_cov3d", [_P, _P, _P]),
@@ -392,12 +393,18 @@ def bvh_build(means, scales):
     return nodes[:k], idx[:n], k - 1 if k > 0 else -1, codes[:n]
 
 
-def raycast(nodes, splat_index, root, means, scales, origin, direction, max_dist=1000.0):
-    """raycast_closest_splat for one ray: a RAY_HIT_DTYPE record."""
+def raycast(nodes, splat_index, root, means, scales, origin, direction, max_dist=1000.0, unit=False):
+    """raycast_closest_splat for one ray: a RAY_HIT_DTYPE record. The ray is
+    Ray3f(origin, direction), which normalises the direction; unit=True
+    passes a Ray3f's stored direction (from generate_ray) as it is."""
     m, s = _f32(means).reshape(-1, 3), _f32(scales).reshape(-1, 3)
     nd = np.ascontiguousarray(nodes, BVH_NODE_DTYPE)
     si = np.ascontiguousarray(splat_index, np.int32)
-    o, d = _f32(origin).reshape(3), _f32(direction).reshape(3)
+    o, d = _f32(origin).reshape(3), _f32(direction).reshape(3).copy()
+    if not unit:
+        dn = np.zeros(3, np.float32)
+        lib().oracle_ray_direction(_ptr(d), _ptr(dn))
+        d = dn
     out = np.zeros(1, RAY_HIT_DTYPE)
     lib().oracle_raycast(nd.ctypes.data, _ptr(si), nd.shape[0], int(root), _ptr(m), _ptr(s), m.shape[0], _ptr(o),
                          _ptr(d), float(max_dist), out.ctypes.data)

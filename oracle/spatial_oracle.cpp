@@ -169,7 +169,11 @@ int64_t oracle_bvh_build(const float* means, const float* scales, int64_t n, voi
     return total;
 }
 
-/* hit_out: LumenRayHit layout (hit, splat index, distance, point xyz). */
+/* Ray3f(origin, direction): the stored direction, normalised (camera.mojo:16-18). */
+void oracle_ray_direction(const float direction[3], float out[3]) { normalize3(direction, out); }
+
+/* hit_out: LumenRayHit layout (hit, splat index, distance, point xyz).
+ * direction: the ray's stored direction (a Ray3f's, already normalised). */
 void oracle_raycast(const void* nodes_in, const int32_t* splat_index, int64_t node_count, int64_t root,
                     const float* means, const float* scales, int64_t n, const float origin[3],
                     const float direction[3], float max_dist, void* hit_out) {
@@ -182,8 +186,7 @@ void oracle_raycast(const void* nodes_in, const int32_t* splat_index, int64_t no
         std::memcpy(hit_out, &h, sizeof(h));
         return;
     }
-    float d[3];
-    normalize3(direction, d);                                /* Ray3f */
+    const float d[3] = {direction[0], direction[1], direction[2]};
     h.distance = max_dist;
     std::vector<int64_t> stack;
     stack.push_back(root);

@@ -52,7 +52,11 @@ def _check(d, near=0.5, far=10.0):
     lo, hi = O.depth_min_max(d)
     r = p.range.cpu().numpy()
     assert r[0] == np.float32(lo) and r[1] == np.float32(hi)
-    assert np.array_equal(p.heatmap.cpu().numpy(), O.depth_heatmap(d, near, far))
+    got_h, want_h = p.heatmap.cpu().numpy(), O.depth_heatmap(d, near, far)
+    bad = np.argwhere((got_h != want_h).any(axis=-1))
+    detail = [(tuple(int(v) for v in b), float(d[tuple(b)]), hex(int(d[tuple(b)].view(np.uint32))),
+               got_h[tuple(b)].tolist(), want_h[tuple(b)].tolist()) for b in bad[:6]]
+    assert bad.shape[0] == 0, f"{bad.shape[0]} heatmap pixels differ: {detail}"
 
 
 @pytest.mark.parametrize("h,w,seed", [(1080, 1920, 0), (13, 17, 1), (1, 1, 2), (1, 300, 3), (257, 1, 4),

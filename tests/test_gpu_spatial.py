@@ -97,7 +97,7 @@ def test_pick_pixels_matches_restatement():
     raw = bvh.pick(cam, _t(px), rays_out=rays)
     want_rays = np.array([np.concatenate(O.generate_ray(cam, x, y)) for x, y in px], np.float32)
     assert np.array_equal(rays.cpu().numpy().view(np.uint32), want_rays.view(np.uint32))
-    want = np.array([O.raycast(nodes, idx, root, sc.means, s, r[:3], r[3:], 1000.0) for r in want_rays],
+    want = np.array([O.raycast(nodes, idx, root, sc.means, s, r[:3], r[3:], 1000.0, unit=True) for r in want_rays],
                     O.RAY_HIT_DTYPE)
     assert want["hit"].sum() > 0
     _compare_hits(raw, want)
