@@ -56,23 +56,4 @@ __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float
     return m;
 }
 
-/* The same test for the forward compositor's four 8x8 pixel blocks (warp
- * w of the 128-thread tile: x offset (w & 1) * 8, y offset (w >> 1) * 8). */
-__device__ __forceinline__ unsigned int reach_mask_8x8(float4 geo, float4 con, float tile_x0, float tile_y0) {
-    const float a = con.x, b = con.y, c = con.z, op = geo.w;
-    if (!(a > 0.0f && c > 0.0f && a * c - b * b > 0.0f) || !isfinite(a * c)) return 0xFu;
-    const float pcut = fminf(4.5f, __logf(op / min_alpha()) + 0.01f);
-    if (pcut < 0.0f) return 0u;
-    const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
-    const float b_over_a = b * __frcp_rn(a), b_over_c = b * __frcp_rn(c);
-    unsigned int m = 0;
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-        const float x0 = tile_x0 + (float)((w & 1) * 8) + 0.5f - geo.x;
-        const float y0 = tile_y0 + (float)((w >> 1) * 8) + 0.5f - geo.y;
-        if (quad_min_rect(a, b, c, b_over_a, b_over_c, x0, x0 + 7.0f, y0, y0 + 7.0f) <= qcut) m |= 1u << w;
-    }
-    return m;
-}
-
 }  // namespace lumen
