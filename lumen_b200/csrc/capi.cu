@@ -48,7 +48,8 @@ struct LumenCloud {
 struct LumenRasterizer {
     LumenConfig config;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t copy_stream = nullptr;   /* uploads the frame buffer while the frame renders */
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_up = nullptr;
     LumenGpuRenderer* renderer = nullptr;
     /* device mirror of the last cloud rendered */
     const LumenCloud* cached_cloud = nullptr;
@@ -201,6 +202,8 @@ void release(LumenRasterizer* r) {
     cudaFree(r->d_rgb); cudaFree(r->d_depth); cudaFree(r->d_alpha); cudaFree(r->d_rgb8);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
+    if (r->ev_up) cudaEventDestroy(r->ev_up);
+    if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
     if (r->stream) cudaStreamDestroy(r->stream);
 }
 
@@ -336,16 +339,42 @@ LumenCloud* lumen_create_synthetic_sphere(size_t count, float radius) {
     return c;
 }
 
+/* The library owns a frame buffer's arrays (lumen.h), so it places them in
+ * page-locked memory when a CUDA device is present: lumen_rasterize's
+ * upload of the old contents and read-back of the new run at the full
+ * host-link rate and asynchronously. Without a device they are plain heap
+ * memory. Which one was used is kept after the struct (the caller holds
+ * only the pointer returned here). */
+struct FrameBufferBlock {
+    LumenFrameBuffer fb;
+    int page_locked;
+};
+
 LumenFrameBuffer* lumen_framebuffer_create(uint32_t width, uint32_t height) {
     if (width == 0 || height == 0) return nullptr;
-    LumenFrameBuffer* fb = (LumenFrameBuffer*)std::malloc(sizeof(LumenFrameBuffer));
-    if (!fb) return nullptr;
+    FrameBufferBlock* blk = (FrameBufferBlock*)std::calloc(1, sizeof(FrameBufferBlock));
+    if (!blk) return nullptr;
+    LumenFrameBuffer* fb = &blk->fb;
     fb->width = width;
     fb->height = height;
     const size_t n = (size_t)width * (size_t)height;
-    fb->rgb_data = (uint8_t*)std::malloc(n * 3);
-    fb->depth_data = (float*)std::malloc(n * sizeof(float));
-    fb->alpha_data = (float*)std::malloc(n * sizeof(float));
+    void *rgb = nullptr, *depth = nullptr, *alpha = nullptr;
+    if (cudaHostAlloc(&rgb, n * 3, cudaHostAllocPortable) == cudaSuccess &&
+        cudaHostAlloc(&depth, n * sizeof(float), cudaHostAllocPortable) == cudaSuccess &&
+        cudaHostAlloc(&alpha, n * sizeof(float), cudaHostAllocPortable) == cudaSuccess) {
+        blk->page_locked = 1;
+    } else {
+        cudaFreeHost(rgb);
+        cudaFreeHost(depth);
+        cudaGetLastError();
+        rgb = std::malloc(n * 3);
+        depth = std::malloc(n * sizeof(float));
+        alpha = std::malloc(n * sizeof(float));
+        blk->page_locked = 0;
+    }
+    fb->rgb_data = (uint8_t*)rgb;
+    fb->depth_data = (float*)depth;
+    fb->alpha_data = (float*)alpha;
     if (!fb->rgb_data || !fb->depth_data || !fb->alpha_data) {
         lumen_framebuffer_destroy(fb);
         return nullptr;
@@ -356,10 +385,17 @@ LumenFrameBuffer* lumen_framebuffer_create(uint32_t width, uint32_t height) {
 
 void lumen_framebuffer_destroy(LumenFrameBuffer* fb) {
     if (!fb) return;
-    std::free(fb->rgb_data);
-    std::free(fb->depth_data);
-    std::free(fb->alpha_data);
-    std::free(fb);
+    FrameBufferBlock* blk = reinterpret_cast<FrameBufferBlock*>(fb);
+    if (blk->page_locked) {
+        cudaFreeHost(fb->rgb_data);
+        cudaFreeHost(fb->depth_data);
+        cudaFreeHost(fb->alpha_data);
+    } else {
+        std::free(fb->rgb_data);
+        std::free(fb->depth_data);
+        std::free(fb->alpha_data);
+    }
+    std::free(blk);
 }
 
 void lumen_framebuffer_clear(LumenFrameBuffer* fb, uint8_t r, uint8_t g, uint8_t b) {
@@ -379,7 +415,9 @@ LumenRasterizer* lumen_rasterizer_create(const LumenConfig* config) {
     if (!r) return nullptr;
     r->config = config ? *config : lumen_default_config();
     if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_up, cudaEventDisableTiming) != cudaSuccess ||
         !(r->renderer = lumen_gpu_renderer_create())) {
         release(r);
         delete r;
@@ -435,14 +473,23 @@ LumenStatus lumen_rasterize(LumenRasterizer* r, const LumenCloud* cloud, const L
     std::memset(&img, 0, sizeof(img));
     img.rgb = r->d_rgb; img.depth = r->d_depth; img.alpha = r->d_alpha;
 
+    /* the old contents (the background) are uploaded on the copy stream
+     * while the frame renders, and joined just before they are blended */
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(r->d_rgb8, fb->rgb_data, npix * 3, cudaMemcpyHostToDevice, r->stream)) != cudaSuccess ||
+    if ((e = cudaStreamWaitEvent(r->copy_stream, r->ev0, 0)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(r->d_rgb8, fb->rgb_data, npix * 3, cudaMemcpyHostToDevice, r->copy_stream)) !=
+            cudaSuccess ||
         (e = cudaMemcpyAsync(r->d_depth + npix, fb->depth_data, npix * sizeof(float), cudaMemcpyHostToDevice,
-                             r->stream)) != cudaSuccess)
+                             r->copy_stream)) != cudaSuccess ||
+        (e = cudaEventRecord(r->ev_up, r->copy_stream)) != cudaSuccess)
         return cuda_status(e);
     LumenGpuCounts counts;
     st = lumen_gpu_renderer_render(r->renderer, &g, &cam, &opt, &img, &counts, r->stream);
-    if (st != LUMEN_SUCCESS) return st;
+    if (st != LUMEN_SUCCESS) {
+        cudaStreamSynchronize(r->copy_stream);
+        return st;
+    }
+    if ((e = cudaStreamWaitEvent(r->stream, r->ev_up, 0)) != cudaSuccess) return cuda_status(e);
     to_framebuffer_kernel<<<1024, 256, 0, r->stream>>>(r->d_rgb, r->d_depth, r->d_alpha, r->d_rgb8,
                                                         r->d_depth + npix, (long long)npix);
     if ((e = cudaMemcpyAsync(fb->rgb_data, r->d_rgb8, npix * 3, cudaMemcpyDeviceToHost, r->stream)) != cudaSuccess ||
