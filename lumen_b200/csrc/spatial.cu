@@ -14,15 +14,17 @@
  *                       reduced with atomicMax on order-preserving bit keys
  *   K2 morton_kernel    one 30-bit code per Gaussian, index as the value
  *   K3 the library's stable onesweep radix sort (32-bit keys, 4 digit passes)
- *   K4 bvh_refit_kernel one thread per leaf writes its leaf, then climbs: at
- *                       each parent with two children the second thread to
- *                       arrive (an atomic counter per parent) builds it from
- *                       both children, the first stops. No thread waits for
- *                       another, and each parent is built exactly once in the
+ *   K4 bvh_levels_kernel, once per ten levels: a block writes 1024 leaves
+ *                       (or loads 1024 nodes of the level reached so far)
+ *                       and builds their ancestors ten levels up in shared
+ *                       memory, one barrier per level. Parents pair adjacent
+ *                       nodes, so 1024 aligned nodes never need another
+ *                       block's: each parent is built once, in the
  *                       reference's order (left box expanded by the right),
- *                       so the nodes equal the reference's level-by-level
- *                       pairing bit for bit. Node numbering is the
- *                       reference's: leaves, then each level's parents.
+ *                       and the nodes equal the reference's level-by-level
+ *                       pairing bit for bit (1M leaves: two launches).
+ *                       Node numbering is the reference's: leaves, then each
+ *                       level's parents.
  * Casts: one thread per ray, the reference's depth-first traversal with its
  * stack order (left pushed before right) and its pruning against the
  * closest hit so far, so hits agree bit for bit, ties included.
@@ -64,7 +66,7 @@ struct BvhLevels {
 };
 
 struct BvhLayout {
-    size_t control_off, flags_off, keys0_off, vals0_off, keys1_off, vals1_off, lb_off, total;
+    size_t control_off, keys0_off, vals0_off, keys1_off, vals1_off, lb_off, total;
     long long sort_tiles;
     size_t zeroed() const { return keys0_off; }
 };
@@ -95,11 +97,9 @@ long long node_count_of(long long n) {
 
 BvhLayout make_layout(long long n) {
     BvhLayout B;
-    const long long internal = node_count_of(n) - n;
     B.sort_tiles = (n + 256 * kBvhSortItems - 1) / (256 * kBvhSortItems);
     B.control_off = 0;
-    B.flags_off = align_up(sizeof(BvhControl), 256);
-    B.keys0_off = align_up(B.flags_off + (size_t)(internal > 0 ? internal : 1) * sizeof(unsigned int), 256);
+    B.keys0_off = align_up(sizeof(BvhControl), 256);
     B.vals0_off = align_up(B.keys0_off + (size_t)n * 4, 256);
     B.keys1_off = align_up(B.vals0_off + (size_t)n * 4, 256);
     B.vals1_off = align_up(B.keys1_off + (size_t)n * 4, 256);
@@ -239,50 +239,79 @@ __device__ __forceinline__ void expand_point(Box& b, const float p[3]) {
         if (p[c] > b.mx[c]) b.mx[c] = p[c];
 }
 
-__global__ void __launch_bounds__(256)
-bvh_refit_kernel(const float* __restrict__ means, const float* __restrict__ scales, long long n,
-                 const BvhControl* __restrict__ ctrl, const unsigned int* __restrict__ v0,
-                 const unsigned int* __restrict__ v1, LumenBvhNode* nodes, int* __restrict__ splat_index,
-                 unsigned int* flags, BvhLevels lv) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const unsigned int* perm = ctrl->sort.sorted_buffer ? v1 : v0;
-    const long long g = perm[i];
-    /* leaf: position +- 3 x the largest scale (bvh.mojo:78-93) */
-    float r = scales[g * 3 + 0];
-    if (scales[g * 3 + 1] > r) r = scales[g * 3 + 1];
-    if (scales[g * 3 + 2] > r) r = scales[g * 3 + 2];
-    const float r3 = r * 3.0f;
-    Box leaf;
+/* Levels of the hierarchy built per launch: a block takes 1024 consecutive
+ * nodes of level L0 (for L0 = 0 it first writes them as leaves) and builds
+ * their ancestors up to level L0 + 10 in shared memory, one level per
+ * barrier; parents pair adjacent nodes exactly as bvh.mojo:96-117 does, so
+ * a block's subtree never needs another block's nodes. */
+constexpr int kRefitSpan = 10;
+constexpr int kRefitNodes = 1 << kRefitSpan;
+constexpr int kRefitThreads = 256;
+
+__global__ void __launch_bounds__(kRefitThreads)
+bvh_levels_kernel(const float* __restrict__ means, const float* __restrict__ scales, long long n,
+                  const BvhControl* __restrict__ ctrl, const unsigned int* __restrict__ v0,
+                  const unsigned int* __restrict__ v1, LumenBvhNode* __restrict__ nodes,
+                  int* __restrict__ splat_index, BvhLevels lv, int L0) {
+    __shared__ Box cur[kRefitNodes];
+    __shared__ Box nxt[kRefitNodes / 2];
+    const int tid = threadIdx.x;
+    const long long b = blockIdx.x;
+    const long long first = b * kRefitNodes;
+    const long long cnt0 = lv.count[L0];
+    const int m0 = (int)(cnt0 - first < kRefitNodes ? cnt0 - first : kRefitNodes);
+    if (L0 == 0) {
+        const unsigned int* perm = ctrl->sort.sorted_buffer ? v1 : v0;
+        for (int k = tid; k < m0; k += kRefitThreads) {
+            const long long i = first + k;
+            const long long g = perm[i];
+            /* leaf: position +- 3 x the largest scale (bvh.mojo:78-93) */
+            float r = scales[g * 3 + 0];
+            if (scales[g * 3 + 1] > r) r = scales[g * 3 + 1];
+            if (scales[g * 3 + 2] > r) r = scales[g * 3 + 2];
+            const float r3 = r * 3.0f;
+            Box leaf;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const float p = means[g * 3 + c];
-        leaf.mn[c] = p - r3;
-        leaf.mx[c] = p + r3;
+            for (int c = 0; c < 3; ++c) {
+                const float pc = means[g * 3 + c];
+                leaf.mn[c] = pc - r3;
+                leaf.mx[c] = pc + r3;
+            }
+            store_node(nodes + i, leaf, -1, -1);
+            splat_index[i] = (int)g;
+            cur[k] = leaf;
+        }
+    } else {
+        for (int k = tid; k < m0; k += kRefitThreads)
+            cur[k] = load_box_cg(nodes + lv.start[L0] + first + k, nullptr, nullptr);
     }
-    store_node(nodes + i, leaf, -1, -1);
-    splat_index[i] = (int)g;
-    /* climb: parents pair adjacent nodes (bvh.mojo:96-117) */
-    long long j = i;
-    for (int L = 0; L + 1 < lv.n_levels; ++L) {
-        const long long pj = j >> 1;
-        const long long parent = lv.start[L + 1] + pj;
-        const long long left = lv.start[L] + 2 * pj;
-        const bool has_right = 2 * pj + 1 < lv.count[L];
-        if (has_right) {
-            __threadfence();                                  /* this thread's node, before the count */
-            const unsigned int seen = atomicAdd(flags + (parent - n), 1u);
-            if (seen == 0u) return;                           /* the sibling builds the parent */
-            __threadfence();
+    __syncthreads();
+    Box* src = cur;
+    Box* dst = nxt;
+    for (int sft = 1; sft <= kRefitSpan && L0 + sft < lv.n_levels; ++sft) {
+        const int L = L0 + sft;
+        const long long pfirst = first >> sft;                 /* this block's first parent at level L */
+        const long long pend = ((first + kRefitNodes) >> sft) < lv.count[L] ? ((first + kRefitNodes) >> sft)
+                                                                             : lv.count[L];
+        const int np = (int)(pend - pfirst);
+        for (int k = tid; k < np; k += kRefitThreads) {
+            const long long pg = pfirst + k;
+            const long long left = lv.start[L - 1] + 2 * pg;
+            const bool has_right = 2 * pg + 1 < lv.count[L - 1];
+            Box bx = src[2 * k];
+            if (has_right) {
+                expand_point(bx, src[2 * k + 1].mn);           /* AABB3f.expand_box, aabb.mojo:56-58 */
+                expand_point(bx, src[2 * k + 1].mx);
+            }
+            store_node(nodes + lv.start[L] + pg, bx, (int)left, has_right ? (int)(left + 1) : -1);
+            dst[k] = bx;
         }
-        Box b = load_box_cg(nodes + left, nullptr, nullptr);
-        if (has_right) {
-            const Box o = load_box_cg(nodes + left + 1, nullptr, nullptr);
-            expand_point(b, o.mn);                            /* AABB3f.expand_box, aabb.mojo:56-58 */
-            expand_point(b, o.mx);
-        }
-        store_node(nodes + parent, b, (int)left, has_right ? (int)(left + 1) : -1);
-        j = pj;
+        __syncthreads();
+        /* ping-pong: the next level reads what this one wrote (an odd level
+         * writes at most 512 parents, into the smaller buffer) */
+        Box* t = src;
+        src = dst;
+        dst = t;
     }
 }
 
@@ -478,7 +507,6 @@ LumenStatus lumen_gpu_bvh_build(const LumenGpuGaussians* g, LumenGpuBvh* bvh, vo
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char* base = (unsigned char*)scratch;
     BvhControl* ctrl = (BvhControl*)(base + B.control_off);
-    unsigned int* flags = (unsigned int*)(base + B.flags_off);
     unsigned int* k0 = (unsigned int*)(base + B.keys0_off);
     unsigned int* v0 = (unsigned int*)(base + B.vals0_off);
     unsigned int* k1 = (unsigned int*)(base + B.keys1_off);
@@ -494,8 +522,14 @@ LumenStatus lumen_gpu_bvh_build(const LumenGpuGaussians* g, LumenGpuBvh* bvh, vo
     launch_key_stats32(k0, n, &ctrl->sort, sms, s);
     launch_sort32(k0, v0, k1, v1, n, &ctrl->sort, lb, B.sort_tiles, nullptr, nullptr, &ctrl->error_flags,
                   kBvhSortItems, 4, sms, s);
-    bvh_refit_kernel<<<(unsigned int)((n + 255) / 256), 256, 0, s>>>(g->means, g->scales, n, ctrl, v0, v1,
-                                                                    bvh->nodes, bvh->splat_index, flags, lv);
+    for (int L0 = 0; L0 + 1 < lv.n_levels; L0 += kRefitSpan) {
+        const long long blocks = (lv.count[L0] + kRefitNodes - 1) / kRefitNodes;
+        bvh_levels_kernel<<<(unsigned int)blocks, kRefitThreads, 0, s>>>(g->means, g->scales, n, ctrl, v0, v1,
+                                                                         bvh->nodes, bvh->splat_index, lv, L0);
+    }
+    if (lv.n_levels == 1)   /* a single leaf: the kernel writes it without climbing */
+        bvh_levels_kernel<<<1, kRefitThreads, 0, s>>>(g->means, g->scales, n, ctrl, v0, v1, bvh->nodes,
+                                                      bvh->splat_index, lv, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return map_cuda(e);
     unsigned int h_flags = 0;
     e = cudaMemcpyAsync(&h_flags, &ctrl->error_flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s);

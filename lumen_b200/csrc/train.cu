@@ -106,10 +106,14 @@ sq_diff_kernel(const float* __restrict__ pred, const float* __restrict__ target,
     }
 }
 
+/* One warp: each lane sums a strided share of the partials, then a fixed
+ * butterfly (the same order on every call, so the result is deterministic). */
 __global__ void psnr_finish_kernel(const float* __restrict__ partial, int nparts, long long n, float* psnr) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
     float s = 0.0f;
-    for (int b = 0; b < nparts; ++b) s += partial[b];
+    for (int b = threadIdx.x; b < nparts; b += 32) s += partial[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x != 0) return;
     const float mse = s / (float)n;                           /* loss.mojo:38-48 */
     *psnr = mse < (float)1e-10 ? (float)99.99 : (float)-4.3429448 * logf(mse);   /* loss.mojo:51-60 */
 }
