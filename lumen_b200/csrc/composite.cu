@@ -199,6 +199,7 @@ template <int kChunk>
 __global__ void __launch_bounds__(kTilePixels, 6)
 composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplatRecord* __restrict__ records,
                  LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
+    chain_begin();
     __shared__ CompositeSmem<kChunk> s;
     composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, blockIdx.x);
 }
@@ -209,6 +210,7 @@ template <int kChunk>
 __global__ void __launch_bounds__(kTilePixels, 6)
 composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRecord* __restrict__ records,
                             LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
+    chain_begin();
     __shared__ CompositeSmem<kChunk> s;
     const long long total = vt->hdr.total_tiles;
     const int n_views = vt->hdr.n_views;
@@ -227,11 +229,11 @@ static void launch_composite_chunk(const ViewTable* vt, int n_views, const Lumen
                                    const LumenRenderOptions& opt, long long n_tiles, bool persistent, int num_sms,
                                    cudaStream_t st) {
     if (persistent) {
-        composite_persistent_kernel<kChunk><<<6 * num_sms, kTilePixels, 0, st>>>(
-            vt, f.records, f, (long long)f.instance_capacity, ctrl, opt);
+        launch_chained(composite_persistent_kernel<kChunk>, dim3(6 * num_sms), dim3(kTilePixels), 0, st, vt,
+                       (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt);
     } else {
-        composite_kernel<kChunk><<<(unsigned int)n_tiles, kTilePixels, 0, st>>>(
-            vt, n_views, f.records, f, (long long)f.instance_capacity, ctrl, opt);
+        launch_chained(composite_kernel<kChunk>, dim3((unsigned int)n_tiles), dim3(kTilePixels), 0, st, vt, n_views,
+                       (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt);
     }
 }
 

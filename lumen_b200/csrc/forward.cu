@@ -134,6 +134,7 @@ static bool frame_ok(const LumenGpuFrame* f, int64_t n, bool need_radii) {
  * view's device camera (setup_camera) into the table. */
 __global__ void frame_init_kernel(unsigned long long* zero, long long n_words, ViewTable* vt, BatchHeader hdr,
                                   ViewDesc v0, int write_view) {
+    chain_begin();
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_words; i += nthreads) zero[i] = 0ull;
     if (blockIdx.x == 0) {
@@ -196,8 +197,8 @@ void launch_init(const ScratchLayout& L, unsigned char* base, const BatchHeader*
     ViewDesc v{};
     if (hdr) h = *hdr;
     if (v0) v = *v0;
-    frame_init_kernel<<<(int)grid, 256, 0, s>>>((unsigned long long*)base, words, (ViewTable*)(base + L.table_off),
-                                               h, v, v0 != nullptr);
+    launch_chained(frame_init_kernel, dim3((int)grid), dim3(256), 0, s, (unsigned long long*)base, words,
+                   (ViewTable*)(base + L.table_off), h, v, (int)(v0 != nullptr));
 }
 
 static bool launch_ok(const LaunchConfig& lc) {

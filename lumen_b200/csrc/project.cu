@@ -53,6 +53,7 @@ template <bool kPersistent>
 __global__ void __launch_bounds__(kProjThreads)
 project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOptions opt, LumenGpuFrame f,
                Control* ctrl, unsigned long long* lb) {
+    chain_begin();
     __shared__ ProjSmem s;
     extern __shared__ float4 sh_stage[];   /* kProjThreads x 12: the block's SH coefficients */
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -186,6 +187,7 @@ struct EmitSmem {
 template <bool kPersistent>
 __global__ void __launch_bounds__(kEmitThreads)
 emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, unsigned long long* lb) {
+    chain_begin();
     __shared__ EmitSmem s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long V = ctrl->n_visible;
@@ -305,10 +307,11 @@ void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& 
     if (n_blocks <= 0) return;
     if (persistent) {
         const int per_sm = g_project_per_sm > 0 ? g_project_per_sm : 1;
-        project_kernel<true><<<per_sm * num_sms, kProjThreads, kProjStageBytes, st>>>(vt, n_views, opt, f, ctrl, lb);
+        launch_chained(project_kernel<true>, dim3(per_sm * num_sms), dim3(kProjThreads), kProjStageBytes, st, vt,
+                       n_views, opt, f, ctrl, lb);
     } else {
-        project_kernel<false><<<(unsigned int)n_blocks, kProjThreads, kProjStageBytes, st>>>(vt, n_views, opt, f,
-                                                                                             ctrl, lb);
+        launch_chained(project_kernel<false>, dim3((unsigned int)n_blocks), dim3(kProjThreads), kProjStageBytes, st,
+                       vt, n_views, opt, f, ctrl, lb);
     }
 }
 
@@ -317,10 +320,11 @@ void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, uns
     if (n_blocks <= 0) return;
     if (persistent) {
         const int per_sm = g_emit_per_sm > 0 ? g_emit_per_sm : 1;
-        emit_kernel<true><<<per_sm * num_sms, kEmitThreads, 0, st>>>(vt, f, ctrl, lb);
+        launch_chained(emit_kernel<true>, dim3(per_sm * num_sms), dim3(kEmitThreads), 0, st, vt, f, ctrl, lb);
     } else {
-        emit_kernel<false><<<(unsigned int)((n_blocks * kProjThreads + kEmitThreads - 1) / kEmitThreads),
-                              kEmitThreads, 0, st>>>(vt, f, ctrl, lb);
+        launch_chained(emit_kernel<false>,
+                       dim3((unsigned int)((n_blocks * kProjThreads + kEmitThreads - 1) / kEmitThreads)),
+                       dim3(kEmitThreads), 0, st, vt, f, ctrl, lb);
     }
 }
 

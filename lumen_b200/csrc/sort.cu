@@ -50,6 +50,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(256)
 histogram_kernel(const KeyT* __restrict__ keys, long long capacity, SortControl* sc, unsigned int* lb,
                  long long lb_tiles_cap, int tile_keys, int* ranges, const long long* n_range_tiles) {
+    chain_begin();
     constexpr int kBytes = (int)sizeof(KeyT);
     constexpr int kRun = kBytes == 8 ? 8 : 16;           /* 64 bytes of keys per thread and run */
     /* a histogram set per warp (per pair of warps for 8-byte keys, to stay
@@ -166,6 +167,7 @@ template <typename KeyT, int kItems>
 __global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : kItems <= 16 ? 3 : 2) : 2)
 onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                      unsigned int* lb_all, long long lb_tiles_cap, unsigned int* err, int digit) {
+    chain_begin();
     constexpr int kTileKeys = kSortThreads * kItems;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PassSmem<KeyT, kItems>& s = *reinterpret_cast<PassSmem<KeyT, kItems>*>(smem_raw);
@@ -294,6 +296,7 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
 __global__ void __launch_bounds__(256)
 tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, ViewTable* vt,
                    int* ranges, Control* ctrl) {
+    chain_begin();
     const SortControl* sc = &ctrl->tile_sort;
     const long long n_tiles = vt->hdr.total_tiles;
     const int n_views = vt->hdr.n_views;
@@ -387,15 +390,15 @@ template <typename KeyT, int kItems>
 void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                       unsigned int* lb, long long lb_tiles_cap, int* ranges, const long long* n_range_tiles,
                       unsigned int* err, int key_bytes, int num_sms, cudaStream_t st) {
-    histogram_kernel<KeyT><<<num_sms * 4, 256, 0, st>>>(k0, capacity, sc, lb, lb_tiles_cap, kSortThreads * kItems,
-                                                        ranges, n_range_tiles);
+    launch_chained(histogram_kernel<KeyT>, dim3(num_sms * 4), dim3(256), 0, st, (const KeyT*)k0, capacity, sc, lb,
+                   lb_tiles_cap, kSortThreads * kItems, ranges, n_range_tiles);
     const size_t smem = sizeof(PassSmem<KeyT, kItems>);
     /* matches __launch_bounds__: all CTAs resident */
     const int ctas_per_sm = sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : kItems <= 16 ? 3 : 2) : 2;
     const int nd = key_bytes < (int)sizeof(KeyT) ? key_bytes : (int)sizeof(KeyT);
     for (int d = 0; d < nd; ++d)
-        onesweep_pass_kernel<KeyT, kItems><<<num_sms * ctas_per_sm, kSortThreads, smem, st>>>(
-            k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d);
+        launch_chained(onesweep_pass_kernel<KeyT, kItems>, dim3(num_sms * ctas_per_sm), dim3(kSortThreads), smem, st,
+                       k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d);
 }
 
 /* items: keys per thread of a digit pass, 8, 16 or 24 (tiles of 2048, 4096
@@ -429,8 +432,8 @@ void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num
     long long grid = ((long long)f.instance_capacity + 1023) / 1024;
     if (grid < num_sms * 4) grid = num_sms * 4;
     if (grid > (1ll << 20)) grid = 1ll << 20;
-    tile_ranges_kernel<<<(unsigned int)grid, 256, 0, st>>>(f.keys[0], f.keys[1], (long long)f.instance_capacity, vt,
-                                                           f.ranges, ctrl);
+    launch_chained(tile_ranges_kernel, dim3((unsigned int)grid), dim3(256), 0, st, (const unsigned int*)f.keys[0],
+                   (const unsigned int*)f.keys[1], (long long)f.instance_capacity, vt, f.ranges, ctrl);
 }
 
 void launch_key_stats64(const unsigned long long* keys, long long n, SortControl* sc, int num_sms, cudaStream_t st) {

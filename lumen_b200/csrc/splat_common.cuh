@@ -538,4 +538,33 @@ __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int x, uns
     return before + incl - x;
 }
 
+/* Programmatic dependent launch (sm_90 and later): the frame's kernels are
+ * launched with launch_chained, so the hardware may schedule a kernel's
+ * blocks while its predecessor's last blocks still run. chain_begin(), the
+ * first statement of every kernel launched that way, waits until the
+ * predecessor has completed and its writes are visible, then allows the
+ * next kernel to be scheduled in turn: nothing is read or written before
+ * the wait, so the stream order of the results is unchanged; only the
+ * launch latency and the predecessor's tail are hidden. */
+__device__ __forceinline__ void chain_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 }  // namespace lumen
