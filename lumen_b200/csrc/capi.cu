@@ -48,8 +48,9 @@ struct LumenCloud {
 struct LumenRasterizer {
     LumenConfig config;
     cudaStream_t stream = nullptr;
-    cudaStream_t copy_stream = nullptr;   /* uploads the frame buffer while the frame renders */
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_up = nullptr;
+    cudaStream_t copy_stream = nullptr;   /* frame-buffer copies, overlapping the render */
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_up = nullptr, ev_down = nullptr;
+    cudaEvent_t ev_band[8] = {};          /* one per compositor band (kRasterBands) */
     LumenGpuRenderer* renderer = nullptr;
     /* device mirror of the last cloud rendered */
     const LumenCloud* cached_cloud = nullptr;
@@ -60,12 +61,16 @@ struct LumenRasterizer {
     /* device image buffers */
     size_t img_cap = 0;
     float* d_rgb = nullptr;
-    float* d_depth = nullptr;
+    float* d_depth = nullptr;             /* rendered | old (uploaded) | out, npix each */
     float* d_alpha = nullptr;
-    unsigned char* d_rgb8 = nullptr;
+    unsigned char* d_rgb8 = nullptr;      /* old (uploaded) | out, npix * 3 each */
 };
 
 namespace lumen {
+
+LumenStatus renderer_render_banded(LumenGpuRenderer* r, const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                   const LumenRenderOptions* opt, LumenGpuImage* img, LumenGpuCounts* counts,
+                                   int n_bands, BandHook hook, void* ctx, cudaStream_t stream);
 
 /* AoS LumenGaussian (59 floats) to the five SoA arrays the kernels read. */
 __global__ void aos_to_soa_kernel(const float* __restrict__ aos, long long n, float* __restrict__ means,
@@ -85,20 +90,24 @@ __global__ void aos_to_soa_kernel(const float* __restrict__ aos, long long n, fl
 }
 
 /* Float image to the 8-bit frame buffer, compositing over its old contents. */
+/* Pixels [p0, p1) of the frame buffer: the render over the old contents
+ * (old colour weighted by the transmittance; the rendered depth where
+ * anything was blended, the old depth elsewhere). */
 __global__ void to_framebuffer_kernel(const float* __restrict__ rgb, const float* __restrict__ depth,
-                                      const float* __restrict__ alpha, unsigned char* __restrict__ rgb8,
-                                      float* __restrict__ depth_out, long long npix) {
+                                      const float* __restrict__ alpha, const unsigned char* __restrict__ old8,
+                                      const float* __restrict__ old_depth, unsigned char* __restrict__ out8,
+                                      float* __restrict__ out_depth, long long p0, long long p1) {
     const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += nthreads) {
+    for (long long p = p0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < p1; p += nthreads) {
         const float a = alpha[p];
         const float T = 1.0f - a;
         for (int c = 0; c < 3; ++c) {
-            float v = rgb[p * 3 + c] + T * ((float)rgb8[p * 3 + c] / 255.0f);
+            float v = rgb[p * 3 + c] + T * ((float)old8[p * 3 + c] / 255.0f);
             if (v < 0.0f) v = 0.0f;
             if (v > 1.0f) v = 1.0f;
-            rgb8[p * 3 + c] = (unsigned char)(v * 255.0f);
+            out8[p * 3 + c] = (unsigned char)(v * 255.0f);
         }
-        if (a > 0.0f) depth_out[p] = depth[p];
+        out_depth[p] = a > 0.0f ? depth[p] : old_depth[p];
     }
 }
 
@@ -189,11 +198,61 @@ LumenStatus ensure_image(LumenRasterizer* r, size_t npix) {
     r->img_cap = 0;
     cudaError_t e;
     if ((e = cudaMalloc(&r->d_rgb, npix * 3 * sizeof(float))) != cudaSuccess) return cuda_status(e);
-    if ((e = cudaMalloc(&r->d_depth, npix * 2 * sizeof(float))) != cudaSuccess) return cuda_status(e);
+    if ((e = cudaMalloc(&r->d_depth, npix * 3 * sizeof(float))) != cudaSuccess) return cuda_status(e);
     if ((e = cudaMalloc(&r->d_alpha, npix * sizeof(float))) != cudaSuccess) return cuda_status(e);
-    if ((e = cudaMalloc(&r->d_rgb8, npix * 3)) != cudaSuccess) return cuda_status(e);
+    if ((e = cudaMalloc(&r->d_rgb8, npix * 6)) != cudaSuccess) return cuda_status(e);
     r->img_cap = npix;
     return LUMEN_SUCCESS;
+}
+
+bool create_band_events(LumenRasterizer* r) {
+    for (cudaEvent_t& ev : r->ev_band)
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return false;
+    return true;
+}
+
+/* Compositor row bands of lumen_rasterize: after each band the render
+ * stream blends the band's rows over the old contents (a short kernel), and
+ * the copy stream reads them back while the next band is composited (the
+ * copy engines need no SM, so the read-back is not held up by the
+ * compositor's blocks). */
+constexpr int kRasterBands = 8;
+
+struct BandCopy {
+    LumenRasterizer* r;
+    LumenFrameBuffer* fb;
+    size_t npix;
+    int next;
+    cudaError_t err;
+};
+
+void band_copy_hook(void* vctx, int y0, int y1, cudaStream_t main) {
+    BandCopy* c = static_cast<BandCopy*>(vctx);
+    if (c->err != cudaSuccess || y1 <= y0) return;
+    LumenRasterizer* r = c->r;
+    const size_t npix = c->npix;
+    const size_t p0 = (size_t)y0 * c->fb->width, p1 = (size_t)y1 * c->fb->width;
+    cudaError_t e;
+    if (c->next == 0 && (e = cudaStreamWaitEvent(main, r->ev_up, 0)) != cudaSuccess) {   /* the old contents */
+        c->err = e;
+        return;
+    }
+    unsigned char* out8 = r->d_rgb8 + npix * 3;
+    float* out_depth = r->d_depth + 2 * npix;
+    to_framebuffer_kernel<<<148, 256, 0, main>>>(r->d_rgb, r->d_depth, r->d_alpha, r->d_rgb8, r->d_depth + npix,
+                                                 out8, out_depth, (long long)p0, (long long)p1);
+    cudaEvent_t ev = r->ev_band[c->next++ % kRasterBands];
+    if ((e = cudaEventRecord(ev, main)) != cudaSuccess || (e = cudaStreamWaitEvent(r->copy_stream, ev, 0)) != cudaSuccess) {
+        c->err = e;
+        return;
+    }
+    if ((e = cudaMemcpyAsync(c->fb->rgb_data + p0 * 3, out8 + p0 * 3, (p1 - p0) * 3, cudaMemcpyDeviceToHost,
+                             r->copy_stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(c->fb->depth_data + p0, out_depth + p0, (p1 - p0) * sizeof(float),
+                             cudaMemcpyDeviceToHost, r->copy_stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(c->fb->alpha_data + p0, r->d_alpha + p0, (p1 - p0) * sizeof(float),
+                             cudaMemcpyDeviceToHost, r->copy_stream)) != cudaSuccess)
+        c->err = e;
 }
 
 void release(LumenRasterizer* r) {
@@ -202,7 +261,10 @@ void release(LumenRasterizer* r) {
     cudaFree(r->d_rgb); cudaFree(r->d_depth); cudaFree(r->d_alpha); cudaFree(r->d_rgb8);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
+    if (r->ev_down) cudaEventDestroy(r->ev_down);
     if (r->ev_up) cudaEventDestroy(r->ev_up);
+    for (cudaEvent_t ev : r->ev_band)
+        if (ev) cudaEventDestroy(ev);
     if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
     if (r->stream) cudaStreamDestroy(r->stream);
 }
@@ -417,8 +479,9 @@ LumenRasterizer* lumen_rasterizer_create(const LumenConfig* config) {
     if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_down, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&r->ev_up, cudaEventDisableTiming) != cudaSuccess ||
-        !(r->renderer = lumen_gpu_renderer_create())) {
+        !create_band_events(r) || !(r->renderer = lumen_gpu_renderer_create())) {
         release(r);
         delete r;
         return nullptr;
@@ -473,8 +536,9 @@ LumenStatus lumen_rasterize(LumenRasterizer* r, const LumenCloud* cloud, const L
     std::memset(&img, 0, sizeof(img));
     img.rgb = r->d_rgb; img.depth = r->d_depth; img.alpha = r->d_alpha;
 
-    /* the old contents (the background) are uploaded on the copy stream
-     * while the frame renders, and joined just before they are blended */
+    /* copy stream: the old contents (the background) go up while the frame
+     * renders; after each compositor band, that band's rows are blended over
+     * them and read back while the next band is composited */
     cudaError_t e;
     if ((e = cudaStreamWaitEvent(r->copy_stream, r->ev0, 0)) != cudaSuccess ||
         (e = cudaMemcpyAsync(r->d_rgb8, fb->rgb_data, npix * 3, cudaMemcpyHostToDevice, r->copy_stream)) !=
@@ -484,20 +548,23 @@ LumenStatus lumen_rasterize(LumenRasterizer* r, const LumenCloud* cloud, const L
         (e = cudaEventRecord(r->ev_up, r->copy_stream)) != cudaSuccess)
         return cuda_status(e);
     LumenGpuCounts counts;
-    st = lumen_gpu_renderer_render(r->renderer, &g, &cam, &opt, &img, &counts, r->stream);
-    if (st != LUMEN_SUCCESS) {
+    BandCopy bc{r, fb, npix, 0, cudaSuccess};
+    st = lumen::renderer_render_banded(r->renderer, &g, &cam, &opt, &img, &counts, kRasterBands, band_copy_hook, &bc,
+                                       r->stream);
+    /* the read-back ends before the call returns, whatever happened */
+    if ((e = cudaEventRecord(r->ev_down, r->copy_stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(r->stream, r->ev_down, 0)) != cudaSuccess) {
         cudaStreamSynchronize(r->copy_stream);
+        return cuda_status(e);
+    }
+    if (st != LUMEN_SUCCESS) {
+        cudaStreamSynchronize(r->stream);
         return st;
     }
-    if ((e = cudaStreamWaitEvent(r->stream, r->ev_up, 0)) != cudaSuccess) return cuda_status(e);
-    to_framebuffer_kernel<<<1024, 256, 0, r->stream>>>(r->d_rgb, r->d_depth, r->d_alpha, r->d_rgb8,
-                                                        r->d_depth + npix, (long long)npix);
-    if ((e = cudaMemcpyAsync(fb->rgb_data, r->d_rgb8, npix * 3, cudaMemcpyDeviceToHost, r->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(fb->depth_data, r->d_depth + npix, npix * sizeof(float), cudaMemcpyDeviceToHost,
-                             r->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(fb->alpha_data, r->d_alpha, npix * sizeof(float), cudaMemcpyDeviceToHost,
-                             r->stream)) != cudaSuccess)
-        return cuda_status(e);
+    if (bc.err != cudaSuccess) {
+        cudaStreamSynchronize(r->stream);
+        return cuda_status(bc.err);
+    }
     cudaEventRecord(r->ev1, r->stream);
     if ((e = cudaEventSynchronize(r->ev1)) != cudaSuccess) return cuda_status(e);
     float ms = 0.0f;

@@ -198,10 +198,11 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
 template <int kChunk>
 __global__ void __launch_bounds__(kTilePixels, 6)
 composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplatRecord* __restrict__ records,
-                 LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
+                 LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt,
+                 long long tile_offset) {
     chain_begin();
     __shared__ CompositeSmem<kChunk> s;
-    composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, blockIdx.x);
+    composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, tile_offset + blockIdx.x);
 }
 
 /* Persistent form for a grid fixed in advance (a captured graph replayed
@@ -226,26 +227,34 @@ composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRe
 
 template <int kChunk>
 static void launch_composite_chunk(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
-                                   const LumenRenderOptions& opt, long long n_tiles, bool persistent, int num_sms,
-                                   cudaStream_t st) {
+                                   const LumenRenderOptions& opt, long long tile_offset, long long n_tiles,
+                                   bool persistent, int num_sms, cudaStream_t st) {
     if (persistent) {
         launch_chained(composite_persistent_kernel<kChunk>, dim3(6 * num_sms), dim3(kTilePixels), 0, st, vt,
                        (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt);
     } else {
         launch_chained(composite_kernel<kChunk>, dim3((unsigned int)n_tiles), dim3(kTilePixels), 0, st, vt, n_views,
-                       (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt);
+                       (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt, tile_offset);
     }
 }
 
-/* chunk: instances staged per round, one of kCompositeChunks. */
+/* chunk: instances staged per round, one of kCompositeChunks. Plain
+ * launches shade tiles [tile_offset, tile_offset + n_tiles) of the batch;
+ * persistent launches take every tile of the table by ticket. */
 void launch_composite(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
-                      const LumenRenderOptions& opt, long long n_tiles, bool persistent, int chunk, int num_sms,
-                      cudaStream_t st) {
+                      const LumenRenderOptions& opt, long long tile_offset, long long n_tiles, bool persistent,
+                      int chunk, int num_sms, cudaStream_t st) {
     if (n_tiles <= 0) return;
     switch (chunk) {
-        case 128: launch_composite_chunk<128>(vt, n_views, f, ctrl, opt, n_tiles, persistent, num_sms, st); break;
-        case 512: launch_composite_chunk<512>(vt, n_views, f, ctrl, opt, n_tiles, persistent, num_sms, st); break;
-        default: launch_composite_chunk<256>(vt, n_views, f, ctrl, opt, n_tiles, persistent, num_sms, st); break;
+        case 128:
+            launch_composite_chunk<128>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+            break;
+        case 512:
+            launch_composite_chunk<512>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+            break;
+        default:
+            launch_composite_chunk<256>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+            break;
     }
 }
 

@@ -43,8 +43,8 @@ void launch_key_stats64(const unsigned long long* keys, long long n, SortControl
 void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_mode, unsigned long long* out,
                           int num_sms, cudaStream_t st);
 void launch_composite(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
-                      const LumenRenderOptions& opt, long long n_tiles, bool persistent, int chunk, int num_sms,
-                      cudaStream_t st);
+                      const LumenRenderOptions& opt, long long tile_offset, long long n_tiles, bool persistent,
+                      int chunk, int num_sms, cudaStream_t st);
 void configure_sort_kernels();
 
 int device_sm_count() {
@@ -154,7 +154,7 @@ __global__ void frame_init_kernel(unsigned long long* zero, long long n_words, V
  * is the batch's view count, or 0 when only the table knows it. */
 void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRenderOptions& opt,
                      const LumenGpuFrame& f, long long n_slots, long long n_tiles, int n_views, bool persistent,
-                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s) {
+                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite) {
     Control* ctrl = (Control*)(base + L.control_off);
     ViewTable* vt = (ViewTable*)(base + L.table_off);
     unsigned long long* proj_lb = (unsigned long long*)(base + L.proj_lb_off);
@@ -183,7 +183,8 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
     if (ev) cudaEventRecord(ev[2], s);
     launch_ranges(f, ctrl, vt, sms, s);
     if (ev) cudaEventRecord(ev[3], s);
-    launch_composite(vt, n_views, f, ctrl, opt, n_tiles, persistent, lc.composite_chunk, sms, s);
+    if (!with_composite) return;
+    launch_composite(vt, n_views, f, ctrl, opt, 0, n_tiles, persistent, lc.composite_chunk, sms, s);
     if (ev) cudaEventRecord(ev[4], s);
 }
 
@@ -235,7 +236,51 @@ static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamer
     v.inst_begin = -1;
     if (ev) cudaEventRecord(ev[0], s);
     launch_init(L, base, &hdr, &v, s);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s, true);
+    return map_cuda(cudaGetLastError());
+}
+
+/* The forward of one view with the compositor launched in n_bands row
+ * bands of tiles; after each band, after_band(ctx, pixel_row_begin,
+ * pixel_row_end, stream) may enqueue work that reads those rows of the
+ * image (copies overlapping the next band). */
+LumenStatus forward_banded(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
+                           LumenGpuFrame* f, LumenGpuImage* img, int n_bands, BandHook after_band, void* ctx,
+                           cudaStream_t s) {
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    if (!img || (!img->rgb && !img->rgb8) || !frame_ok(f, g->count, true) || n_bands < 1)
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    const ScratchLayout L = ScratchLayout::make(g->count, f->instance_capacity);
+    if (f->scratch_bytes < L.total) return LUMEN_ERROR_INVALID_ARGUMENT;
+    configure_once();
+    unsigned char* base = (unsigned char*)f->scratch;
+    const int tiles_x = (cam->width + kTile - 1) / kTile;
+    const int tiles_y = (cam->height + kTile - 1) / kTile;
+    const long long tiles = (long long)tiles_x * tiles_y;
+    BatchHeader hdr{};
+    hdr.n_views = 1;
+    hdr.total_blocks = L.proj_blocks;
+    hdr.total_tiles = tiles;
+    ViewDesc v{};
+    v.g = *g;
+    v.cam = *cam;
+    v.tiles_x = tiles_x;
+    v.img = *img;
+    v.inst_begin = -1;
+    launch_init(L, base, &hdr, &v, s);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, nullptr, s, false);
+    Control* ctrl = (Control*)(base + L.control_off);
+    const ViewTable* vt = (const ViewTable*)(base + L.table_off);
+    const int sms = device_sm_count();
+    if (n_bands > tiles_y) n_bands = tiles_y;
+    for (int b = 0; b < n_bands; ++b) {
+        const int r0 = (int)((long long)tiles_y * b / n_bands), r1 = (int)((long long)tiles_y * (b + 1) / n_bands);
+        launch_composite(vt, 1, *f, ctrl, *opt, (long long)r0 * tiles_x, (long long)(r1 - r0) * tiles_x, false,
+                         kDefaultLaunch.composite_chunk, sms, s);
+        const int y0 = r0 * kTile, y1 = r1 * kTile < cam->height ? r1 * kTile : cam->height;
+        if (after_band) after_band(ctx, y0, y1, s);
+    }
     return map_cuda(cudaGetLastError());
 }
 
@@ -299,7 +344,7 @@ static LumenStatus batch_impl(const LumenGpuBatchView* views, int n_views, const
     cudaError_t e = cudaMemcpyAsync(base + L.table_off, host.data(), host.size(), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return map_cuda(e);
     launch_init(L, base, nullptr, nullptr, s);
-    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, kDefaultLaunch, ev, s);
+    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, kDefaultLaunch, ev, s, true);
     return map_cuda(cudaGetLastError());
 }
 
@@ -606,3 +651,36 @@ LumenStatus lumen_gpu_renderer_render(LumenGpuRenderer* r, const LumenGpuGaussia
 }
 
 }  // extern "C"
+
+namespace lumen {
+
+/* lumen_gpu_renderer_render with the compositor in row bands
+ * (forward_banded): the whole frame is enqueued, bands and hooks included,
+ * before the one host wait for the counts; on a capacity overflow the
+ * buffers grow and the frame, hooks included, is enqueued again. */
+LumenStatus renderer_render_banded(LumenGpuRenderer* r, const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                   const LumenRenderOptions* opt, LumenGpuImage* img, LumenGpuCounts* counts,
+                                   int n_bands, BandHook hook, void* ctx, cudaStream_t stream) {
+    if (!r) return LUMEN_ERROR_INVALID_ARGUMENT;
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    const int64_t tiles = (int64_t)((cam->width + kTile - 1) / kTile) * ((cam->height + kTile - 1) / kTile);
+    const int64_t k_guess = r->k_cap > 0 ? r->k_cap : (g->count * 8 > (1 << 20) ? g->count * 8 : (1 << 20));
+    st = ensure(r, g->count > 0 ? g->count : 1, tiles, k_guess);
+    if (st != LUMEN_SUCCESS) return st;
+    LumenGpuCounts c;
+    std::memset(&c, 0, sizeof(c));
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        st = forward_banded(g, cam, opt, &r->frame, img, n_bands, hook, ctx, stream);
+        if (st != LUMEN_SUCCESS) return st;
+        st = lumen_gpu_read_counts(&r->frame, &c, stream);
+        if (st != LUMEN_SUCCESS) return st;
+        if (!(c.error_flags & LUMEN_GPU_ERR_CAPACITY)) break;
+        st = ensure(r, g->count, tiles, c.n_instances);
+        if (st != LUMEN_SUCCESS) return st;
+    }
+    if (counts) *counts = c;
+    return status_from_flags(c.error_flags);
+}
+
+}  // namespace lumen

@@ -41,7 +41,7 @@ void launch_init(const ScratchLayout& L, unsigned char* base, const BatchHeader*
                  cudaStream_t s);
 void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRenderOptions& opt,
                      const LumenGpuFrame& f, long long n_slots, long long n_tiles, int n_views, bool persistent,
-                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s);
+                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite);
 
 namespace {
 
@@ -236,7 +236,7 @@ void enqueue_batch_work(LumenServer* srv, Slot* s, const LaunchConfig& lc, bool 
     cudaMemcpyAsync(base + s->layout.table_off, s->h_table, table_bytes, cudaMemcpyHostToDevice, s->stream);
     launch_init(s->layout, base, nullptr, nullptr, s->stream);
     launch_pipeline(s->layout, base, srv->cfg.options, s->frame, n_slots, n_tiles, n_views, persistent, lc, nullptr,
-                    s->stream);
+                    s->stream, true);
     cudaMemcpyAsync(s->h_back, base + s->layout.control_off, sizeof(Control), cudaMemcpyDeviceToHost, s->stream);
     cudaMemcpyAsync(s->h_back + sizeof(Control), base + s->layout.table_off, table_bytes, cudaMemcpyDeviceToHost,
                     s->stream);

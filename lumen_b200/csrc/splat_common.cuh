@@ -567,4 +567,8 @@ inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 bloc
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+/* Host hook called after each row band of a banded frame has been
+ * enqueued (pixel rows [row_begin, row_end)). */
+using BandHook = void (*)(void* ctx, int row_begin, int row_end, cudaStream_t s);
+
 }  // namespace lumen
