@@ -123,6 +123,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                           const float* __restrict__ out_alpha, const float* __restrict__ grad_rgb,
                           const float* __restrict__ grad_depth, const float* __restrict__ grad_alpha,
                           float* __restrict__ grad2d) {
+    chain_begin();
     __shared__ BackwardSmem s;
     const int tile = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -301,6 +302,7 @@ __device__ __forceinline__ void sh_term(int k, float x, float y, float z, float&
 __global__ void __launch_bounds__(256, 3)
 project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt,
                         const int* __restrict__ radii, const float* __restrict__ grad2d, LumenGpuGradients out) {
+    chain_begin();
     __shared__ DevCamera cam_s;
     if (threadIdx.x == 0) setup_camera(camera, cam_s);
     __syncthreads();
@@ -535,6 +537,7 @@ constexpr int kL1Blocks = 1024;
 __global__ void __launch_bounds__(256)
 l1_loss_kernel(const float* __restrict__ pred, const float* __restrict__ target, long long n,
                float* __restrict__ grad, float* __restrict__ partial) {
+    chain_begin();
     __shared__ float ws[8];
     const float inv_n = 1.0f / (float)n;
     float sum = 0.0f;
@@ -556,6 +559,7 @@ l1_loss_kernel(const float* __restrict__ pred, const float* __restrict__ target,
 }
 
 __global__ void l1_finish_kernel(const float* __restrict__ partial, long long n, float* loss) {
+    chain_begin();
     __shared__ float ws[32];
     float t = 0.0f;
     for (int b = threadIdx.x; b < kL1Blocks; b += blockDim.x) t += partial[b];
@@ -599,11 +603,13 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenVie
     if (e != cudaSuccess) return map_cuda(e);
     const int tiles_x = (cam->width + kTile - 1) / kTile;
     const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
-    composite_backward_kernel<<<tiles, kTilePixels, 0, s>>>(f->records, *f, ctrl, cam->width, cam->height, tiles_x,
-                                                            *opt, fwd->rgb, fwd->depth, fwd->alpha, grad_rgb,
-                                                            grad_depth, grad_alpha, out->splat2d);
+    launch_chained(composite_backward_kernel, dim3(tiles), dim3(kTilePixels), 0, s,
+                   (const LumenSplatRecord*)f->records, *f, ctrl, cam->width, cam->height, tiles_x, *opt,
+                   (const float*)fwd->rgb, (const float*)fwd->depth, (const float*)fwd->alpha, grad_rgb, grad_depth,
+                   grad_alpha, out->splat2d);
     const long long nb = (g->count + 255) / 256;
-    project_backward_kernel<<<(unsigned int)nb, 256, 0, s>>>(*g, *cam, *opt, f->radii, out->splat2d, *out);
+    launch_chained(project_backward_kernel, dim3((unsigned int)nb), dim3(256), 0, s, *g, *cam, *opt,
+                   (const int*)f->radii, (const float*)out->splat2d, *out);
     return map_cuda(cudaGetLastError());
 }
 
@@ -615,11 +621,11 @@ LumenStatus lumen_gpu_l1_loss(const float* pred, const float* target, int64_t n,
     cudaStream_t s = (cudaStream_t)stream;
     float* partial = (float*)scratch;
     if (n > 0) {
-        l1_loss_kernel<<<kL1Blocks, 256, 0, s>>>(pred, target, n, grad, partial);
+        launch_chained(l1_loss_kernel, dim3(kL1Blocks), dim3(256), 0, s, pred, target, (long long)n, grad, partial);
     } else {
         cudaMemsetAsync(partial, 0, lumen_gpu_l1_loss_scratch_bytes(), s);
     }
-    l1_finish_kernel<<<1, 256, 0, s>>>(partial, n, loss);
+    launch_chained(l1_finish_kernel, dim3(1), dim3(256), 0, s, (const float*)partial, (long long)n, loss);
     return map_cuda(cudaGetLastError());
 }
 

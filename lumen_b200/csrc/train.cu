@@ -39,6 +39,7 @@ adam_kernel(float* __restrict__ means, float* __restrict__ opac, const float* __
             const float* __restrict__ gop, float* __restrict__ m_pos, float* __restrict__ v_pos,
             float* __restrict__ m_op, float* __restrict__ v_op, long long n, float pos_lr, float opacity_lr,
             float b1, float b2, float eps, float ib1, float ib2) {
+    chain_begin();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
 #pragma unroll
@@ -70,6 +71,7 @@ adam_kernel(float* __restrict__ means, float* __restrict__ opac, const float* __
 __global__ void __launch_bounds__(256)
 viewspace_kernel(const float* __restrict__ g2d, int stride_f, const int* __restrict__ radii, long long n,
                  float sx, float sy, float* __restrict__ sum, int* __restrict__ count) {
+    chain_begin();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         if (radii[i] <= 0) continue;
@@ -88,6 +90,7 @@ __global__ void reset_kernel(float* __restrict__ op, long long n, float max_valu
 __global__ void __launch_bounds__(256)
 sq_diff_kernel(const float* __restrict__ pred, const float* __restrict__ target, long long n,
                float* __restrict__ partial) {
+    chain_begin();
     __shared__ float ws[8];
     float sum = 0.0f;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -109,6 +112,7 @@ sq_diff_kernel(const float* __restrict__ pred, const float* __restrict__ target,
 /* One warp: each lane sums a strided share of the partials, then a fixed
  * butterfly (the same order on every call, so the result is deterministic). */
 __global__ void psnr_finish_kernel(const float* __restrict__ partial, int nparts, long long n, float* psnr) {
+    chain_begin();
     float s = 0.0f;
     for (int b = threadIdx.x; b < nparts; b += 32) s += partial[b];
 #pragma unroll
@@ -306,9 +310,10 @@ LumenStatus lumen_gpu_adam_step(LumenGpuGaussians* g, const float* grad_means, c
     const float ib1 = 1.0f / (1.0f - powf(b1, t));
     const float ib2 = 1.0f / (1.0f - powf(b2, t));
     if (g->count == 0) return LUMEN_SUCCESS;
-    adam_kernel<<<grid_for(g->count), 256, 0, (cudaStream_t)stream>>>(
-        const_cast<float*>(g->means), const_cast<float*>(g->opacities), grad_means, grad_op, st->m_pos, st->v_pos,
-        st->m_opacity, st->v_opacity, g->count, pos_lr, c->opacity_lr, b1, b2, eps, ib1, ib2);
+    launch_chained(adam_kernel, dim3(grid_for(g->count)), dim3(256), 0, (cudaStream_t)stream,
+                   const_cast<float*>(g->means), const_cast<float*>(g->opacities), grad_means, grad_op, st->m_pos,
+                   st->v_pos, st->m_opacity, st->v_opacity, (long long)g->count, pos_lr, c->opacity_lr, b1, b2, eps,
+                   ib1, ib2);
     return map_cuda(cudaGetLastError());
 }
 
@@ -317,8 +322,8 @@ LumenStatus lumen_gpu_accumulate_viewspace(const float* splat2d, int32_t stride,
     if (n < 0 || stride < 2) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (n == 0) return LUMEN_SUCCESS;
     if (!splat2d || !radii || !sum || !count) return LUMEN_ERROR_INVALID_ARGUMENT;
-    viewspace_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(splat2d, stride, radii, n, scale_x, scale_y,
-                                                                     sum, count);
+    launch_chained(viewspace_kernel, dim3(grid_for(n)), dim3(256), 0, (cudaStream_t)stream, splat2d, (int)stride,
+                   (const int*)radii, (long long)n, scale_x, scale_y, sum, (int*)count);
     return map_cuda(cudaGetLastError());
 }
 
@@ -388,8 +393,9 @@ LumenStatus lumen_gpu_psnr(const float* pred, const float* target, int64_t n, fl
     if (n <= 0 || !pred || !target || !psnr || !scratch) return LUMEN_ERROR_INVALID_ARGUMENT;
     cudaStream_t s = (cudaStream_t)stream;
     float* partial = (float*)scratch;
-    sq_diff_kernel<<<kPsnrBlocks, 256, 0, s>>>(pred, target, n, partial);
-    psnr_finish_kernel<<<1, 32, 0, s>>>(partial, kPsnrBlocks, n, psnr);
+    launch_chained(sq_diff_kernel, dim3(kPsnrBlocks), dim3(256), 0, s, pred, target, (long long)n, partial);
+    launch_chained(psnr_finish_kernel, dim3(1), dim3(32), 0, s, (const float*)partial, (int)kPsnrBlocks, (long long)n,
+                   psnr);
     return map_cuda(cudaGetLastError());
 }
 

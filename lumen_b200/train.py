@@ -62,10 +62,13 @@ class Trainer:
         self.step_count = 0
         self._reset_state(n)
         self.frame = None
+        self.capacity = 0
+        self.image = None
         self.l1_scratch = torch.empty(int(self.lib.lumen_gpu_l1_loss_scratch_bytes()), dtype=torch.uint8,
                                       device=self.dev)
-        self.loss = torch.zeros((), device=self.dev)
-        self.psnr = torch.zeros((), device=self.dev)
+        self.psnr_scratch = torch.empty_like(self.l1_scratch)
+        self.metrics_dev = torch.zeros(2, device=self.dev)              # loss, PSNR
+        self.metrics_host = torch.zeros(2).pin_memory() if torch.cuda.is_available() else torch.zeros(2)
         self.last_densify_ms = 0.0
 
     def _reset_state(self, n: int, moments=None):
@@ -90,33 +93,60 @@ class Trainer:
         s.step = step
         return s
 
+    def _images(self, h: int, w: int):
+        if self.image is None or self.image[0].shape[:2] != (h, w):
+            e = lambda *s: torch.empty(s, dtype=torch.float32, device=self.dev)
+            self.image = (e(h, w, 3), e(h, w), e(h, w), e(h, w, 3))        # rgb, depth, alpha, dL/drgb
+        return self.image
+
     def train_step(self, camera: ViewCamera, ground_truth: torch.Tensor, iteration: int) -> TrainingMetrics:
+        """One step with a single host wait: the forward, loss, PSNR and
+        backward are enqueued, then the instance count, loss and PSNR are read
+        together; if the frame outgrew its instance buffers nothing has been
+        updated yet, so the buffers grow and the step is enqueued again.
+        Adam, the accumulation and the scheduled density control follow
+        without another wait (density control reads its counts back)."""
         lib, dev = self.lib, self.dev
         stream = torch.cuda.current_stream(dev).cuda_stream
         n = self.count
-        # 1. forward
-        res = R.render(*self.params, camera, self.options, frame=self.frame)
-        self.frame = res.frame
         gt = ground_truth.to(dev).float().contiguous()
-        if gt.numel() != res.rgb.numel():
+        H, W = int(camera.height), int(camera.width)
+        if gt.numel() != H * W * 3:
             raise L.LumenError(-1, "train_step: ground truth does not match the camera's image size")
-        # 2. loss and PSNR
-        gimg = torch.empty_like(res.rgb)
-        L.check(lib.lumen_gpu_l1_loss(res.rgb.data_ptr(), gt.data_ptr(), res.rgb.numel(), gimg.data_ptr(),
-                                      self.loss.data_ptr(), self.l1_scratch.data_ptr(), stream), "l1_loss")
-        L.check(lib.lumen_gpu_psnr(res.rgb.data_ptr(), gt.data_ptr(), res.rgb.numel(), self.psnr.data_ptr(),
-                                   self.l1_scratch.data_ptr(), stream), "psnr")
-        # 3. backward
-        out = L.LumenGpuGradients()
-        out.means, out.scales, out.quats, out.opacities, out.sh = (g.data_ptr() for g in self.grads)
-        out.splat2d = self.splat2d.data_ptr()
-        fwd = L.LumenGpuImage()
-        fwd.rgb, fwd.depth, fwd.alpha = res.rgb.data_ptr(), res.depth.data_ptr(), res.alpha.data_ptr()
+        rgb, depth, alpha, gimg = self._images(H, W)
         g = self._gaussians()
         cam, opt = L.view_camera(camera), L.render_options(self.options)
-        fs = res.frame.c_struct()
-        L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(cam), C.byref(opt), C.byref(fs), C.byref(fwd),
-                                              gimg.data_ptr(), None, None, C.byref(out), stream), "backward")
+        img = L.LumenGpuImage()
+        img.rgb, img.depth, img.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
+        out = L.LumenGpuGradients()
+        out.means, out.scales, out.quats, out.opacities, out.sh = (t.data_ptr() for t in self.grads)
+        out.splat2d = self.splat2d.data_ptr()
+        tiles = camera.n_tiles
+        counts = L.LumenGpuCounts()
+        for _ in range(2):
+            cap = self.capacity or max(1 << 16, 8 * n)
+            if self.frame is None or not self.frame.fits(n, tiles) or self.frame.capacity < cap:
+                self.frame = R.Frame.allocate(n, tiles, cap, dev)
+            fs = self.frame.c_struct()
+            # 1. forward, 2. L1 loss and PSNR, 3. backward
+            L.check(lib.lumen_gpu_render_forward(C.byref(g), C.byref(cam), C.byref(opt), C.byref(fs), C.byref(img),
+                                                 stream), "render_forward")
+            L.check(lib.lumen_gpu_l1_loss(rgb.data_ptr(), gt.data_ptr(), rgb.numel(), gimg.data_ptr(),
+                                          self.metrics_dev.data_ptr(), self.l1_scratch.data_ptr(), stream), "l1_loss")
+            L.check(lib.lumen_gpu_psnr(rgb.data_ptr(), gt.data_ptr(), rgb.numel(), self.metrics_dev.data_ptr() + 4,
+                                       self.psnr_scratch.data_ptr(), stream), "psnr")
+            L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(cam), C.byref(opt), C.byref(fs), C.byref(img),
+                                                  gimg.data_ptr(), None, None, C.byref(out), stream), "backward")
+            self.metrics_host.copy_(self.metrics_dev, non_blocking=True)
+            L.check(lib.lumen_gpu_read_counts(C.byref(fs), C.byref(counts), stream), "read_counts")   # the wait
+            if not counts.error_flags & L.ERR_CAPACITY:
+                break
+            need = int(counts.n_instances)
+            self.capacity = need + need // 4 + 4096
+        if counts.error_flags:
+            raise L.LumenError(-4 if not counts.error_flags & L.ERR_CAPACITY else -2,
+                               f"train_step device flags {counts.error_flags:#x}")
+        self.capacity = max(self.capacity, self.frame.capacity)
         # 4. Adam on positions and opacity
         st = self._adam_state(self.moments, self.step_count)
         cfg = self.config
@@ -124,18 +154,16 @@ class Trainer:
                                         C.byref(st), C.byref(cfg), stream), "adam_step")
         self.step_count = int(st.step)
         # 5. view-space gradients of the visible Gaussians
-        L.check(lib.lumen_gpu_accumulate_viewspace(self.splat2d.data_ptr(), 12, res.frame.radii.data_ptr(), n,
+        L.check(lib.lumen_gpu_accumulate_viewspace(self.splat2d.data_ptr(), 12, self.frame.radii.data_ptr(), n,
                                                    0.5 * camera.width, 0.5 * camera.height,
                                                    self.vs_sum.data_ptr(), self.vs_count.data_ptr(), stream),
                 "accumulate_viewspace")
-        metrics = TrainingMetrics(iteration, 0.0, 0.0, n)
+        metrics = TrainingMetrics(iteration, float(self.metrics_host[0]), float(self.metrics_host[1]), n)
         # 6. density control and opacity reset
         if lib.lumen_training_should_densify(C.byref(cfg), iteration):
             metrics.cloned, metrics.split, metrics.pruned = self.densify_and_prune()
         if lib.lumen_training_should_reset_opacity(C.byref(cfg), iteration):
             L.check(lib.lumen_gpu_reset_opacities(self.params[3].data_ptr(), self.count, 0.01, stream), "reset")
-        metrics.loss = float(self.loss.item())
-        metrics.psnr = float(self.psnr.item())
         metrics.splat_count = self.count
         return metrics
 
