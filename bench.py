@@ -39,6 +39,9 @@ METRIC = "1080p frames/s and p99 latency, served vs per-call render; fwd+bwd ste
 UNIT = "frames/s"
 N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
+# DRAM bytes (read + write) of one composite_kernel launch at the 1 M-Gaussian
+# 1080p workload, from an ncu capture (profiles/composite_config1.md)
+COMPOSITE_DRAM_BYTES = 42.4e6
 KERNELS_PER_FRAME = 14   # init, project, 2 x (histogram + 4 digit passes), emit, tile_ranges, composite
 
 
@@ -900,7 +903,10 @@ def main():
            "sort": 8 * N_GAUSSIANS + 16 * V + 12 * K + 8 * K + 24 * K * p,
            "tile_ranges": 8 * K + 8 * T,
            "composite": 40 * K + 16 * P}
-    dom = max(range(4), key=lambda i: stage_ms[i])
+    # the dominant kernel: composite_kernel, the largest share of the frame's
+    # launch list (profiles/forward_config1_launches.md); the sort stage is
+    # nine kernels, none above an eighth of the frame
+    dom = names.index("composite")
     dname = names[dom]
     achieved = alg[dname] / (stage_ms[dom] * 1e-3) / 1e9
     b_fwd = 244 * N_GAUSSIANS + 64 * V + (68 + 24 * passes) * K + 8 * T + 16 * P
@@ -916,8 +922,10 @@ def main():
             "stages_timing": "a second run of the K frames with CUDA events between the stages",
             "counts": {"visible": V, "instances": K, "tiles": T, "digit_passes": passes},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
-                         "algorithmic_bytes": alg[dname]},
+                         "frac": achieved / hbm_peak, "traffic": COMPOSITE_DRAM_BYTES, "peak_source": peak_src,
+                         "algorithmic_bytes": alg[dname],
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one composite_kernel "
+                                           "launch at this workload (profiles/composite_config1.md)"},
             "frame_roofline": {"bytes": b_fwd, "achieved": frame_gbs, "peak": hbm_peak, "unit": "GB/s",
                                "frac": frame_gbs / hbm_peak}}
     if not args.no_multiview:

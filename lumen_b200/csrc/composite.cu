@@ -43,6 +43,67 @@ struct CompositeSmem {
     unsigned int ticket;
 };
 
+/* A pixel's front-to-back state (PixelAccumulator, compositor.mojo:10-59). */
+struct PixelState {
+    float T, cr, cg, cb, dep, acc;
+    unsigned int count;
+    int last;
+    bool done;
+};
+
+/* The warp's list of splats of the staged chunk, in sorted order, for the
+ * warp's pixel. kClamp: some staged splat has opacity above 0.99, so the
+ * 0.99 alpha clamp can apply (without one, alpha = opacity * exp(-power)
+ * with exp(-power) <= 1 never exceeds it and the test is left out).
+ * kModeAlpha: stop when 1 - T reaches the threshold, else when T falls to
+ * it. Either way the arithmetic is the reference's, operation by
+ * operation. */
+template <int kChunk, bool kClamp, bool kModeAlpha>
+__device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int warp, int cnt, int cs, float pxc,
+                                           float pyc, float thr, PixelState& p) {
+    for (int t = 0; t < cnt; ++t) {
+        const int j = s.list[warp][t];
+        if (!p.done) {
+            const float4 gg = s.geo[j];
+            const float4 cc = s.con[j];
+            /* compute_gaussian_pixel_alpha, compositor.mojo:62-89 */
+            const float dx = pxc - gg.x;
+            const float dy = pyc - gg.y;
+            float power = cc.x * dx * dx + cc.y * dx * dy + cc.z * dy * dy;
+            bool skip = false;
+            if (power < 0.0f) power = 0.0f;
+            else if (power > 4.5f) skip = true;
+            if (!skip) {
+                float alpha = gg.w * lumen_expf_core(-power);
+                if (kClamp && alpha > (float)0.99) alpha = (float)0.99;
+                /* PixelAccumulator.blend, compositor.mojo:25-53 */
+                if (!(alpha < min_alpha())) {
+                    const float4 col = s.col[j];
+                    const float w = alpha * p.T;
+                    p.cr += col.x * w;
+                    p.cg += col.y * w;
+                    p.cb += col.z * w;
+                    p.dep += gg.z * w;
+                    p.T *= (1.0f - alpha);
+                    ++p.count;
+                    if (kModeAlpha) {
+                        p.acc = 1.0f - p.T;
+                        if (p.acc >= thr) {
+                            p.done = true;
+                            p.last = cs + j;
+                        }
+                    } else if (p.T <= thr) {
+                        p.done = true;
+                        p.last = cs + j;
+                    }
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, p.done)) break;
+    }
+    if (!kModeAlpha) p.acc = 1.0f - p.T;     /* the value the reference's blend leaves (compositor.mojo:51) */
+}
+
 /* One tile of the batch (batch-wide id gtile, owned by the last view whose
  * tile_begin <= gtile). */
 template <int kChunk>
@@ -92,6 +153,7 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
             bool done = !inside;
             for (int cs = rs; cs < re; cs += kChunk) {
                 if (__syncthreads_count(!done) == 0) break;
+                int high = 0;
 #pragma unroll
                 for (int r = 0; r < (kChunk + kTilePixels - 1) / kTilePixels; ++r) {
                     const int slot = r * kTilePixels + tid;
@@ -112,11 +174,14 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
                             s.con[slot] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
                             s.col[slot] = __ldg(r4 + 2);
                             m = reach_mask(geo, con, tile_x0, tile_y0);
+                            high |= geo.w > (float)0.99;
                         }
                     }
                     s.mask[slot] = (unsigned char)m;
                 }
-                __syncthreads();
+                /* whether any staged splat has opacity above 0.99: only those can
+                 * reach the 0.99 alpha clamp (exp(-power) <= 1 for power >= 0) */
+                const bool clamp = __syncthreads_or(high) != 0;
                 /* this warp's splats of the chunk, in sorted order */
                 const int n = re - cs < kChunk ? re - cs : kChunk;
                 int cnt = 0;
@@ -128,41 +193,16 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
                     cnt += __popc(bal);
                 }
                 __syncwarp();
-                for (int t = 0; t < cnt; ++t) {
-                    const int j = s.list[warp][t];
-                    if (!done) {
-                        const float4 gg = s.geo[j];
-                        const float4 cc = s.con[j];
-                        /* compute_gaussian_pixel_alpha, compositor.mojo:62-89 */
-                        const float dx = pxc - gg.x;
-                        const float dy = pyc - gg.y;
-                        float power = cc.x * dx * dx + cc.y * dx * dy + cc.z * dy * dy;
-                        bool skip = false;
-                        if (power < 0.0f) power = 0.0f;
-                        else if (power > 4.5f) skip = true;
-                        if (!skip) {
-                            float alpha = gg.w * lumen_expf_core(-power);
-                            if (alpha > (float)0.99) alpha = (float)0.99;
-                            /* PixelAccumulator.blend, compositor.mojo:25-53 */
-                            if (!(alpha < min_alpha())) {
-                                const float4 col = s.col[j];
-                                const float w = alpha * T;
-                                cr += col.x * w;
-                                cg += col.y * w;
-                                cb += col.z * w;
-                                dep += gg.z * w;
-                                T *= (1.0f - alpha);
-                                acc = 1.0f - T;
-                                ++count;
-                                if (mode_alpha ? (acc >= thr) : (T <= thr)) {
-                                    done = true;
-                                    last = cs + j;
-                                }
-                            }
-                        }
-                    }
-                    if (__all_sync(0xffffffffu, done)) break;
+                PixelState px_state{T, cr, cg, cb, dep, acc, count, last, done};
+                if (clamp) {
+                    if (mode_alpha) blend_list<kChunk, true, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    else blend_list<kChunk, true, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                } else {
+                    if (mode_alpha) blend_list<kChunk, false, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    else blend_list<kChunk, false, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
                 }
+                T = px_state.T; cr = px_state.cr; cg = px_state.cg; cb = px_state.cb; dep = px_state.dep;
+                acc = px_state.acc; count = px_state.count; last = px_state.last; done = px_state.done;
                 __syncthreads();
             }
             /* a pixel that never saturated visited the whole range */
