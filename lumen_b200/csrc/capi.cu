@@ -50,7 +50,7 @@ struct LumenRasterizer {
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;   /* frame-buffer copies, overlapping the render */
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_up = nullptr, ev_down = nullptr;
-    cudaEvent_t ev_band[8] = {};          /* one per compositor band (kRasterBands) */
+    cudaEvent_t ev_band[4] = {};          /* one per compositor band (kRasterBands) */
     LumenGpuRenderer* renderer = nullptr;
     /* device mirror of the last cloud rendered */
     const LumenCloud* cached_cloud = nullptr;
@@ -216,7 +216,7 @@ bool create_band_events(LumenRasterizer* r) {
  * the copy stream reads them back while the next band is composited (the
  * copy engines need no SM, so the read-back is not held up by the
  * compositor's blocks). */
-constexpr int kRasterBands = 8;
+constexpr int kRasterBands = 4;
 
 struct BandCopy {
     LumenRasterizer* r;

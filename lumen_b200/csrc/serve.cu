@@ -234,9 +234,13 @@ void enqueue_batch_work(LumenServer* srv, Slot* s, const LaunchConfig& lc, bool 
                         long long n_tiles, int n_views, size_t table_bytes) {
     unsigned char* base = (unsigned char*)s->frame.scratch;
     cudaMemcpyAsync(base + s->layout.table_off, s->h_table, table_bytes, cudaMemcpyHostToDevice, s->stream);
-    launch_init(s->layout, base, nullptr, nullptr, s->stream);
-    launch_pipeline(s->layout, base, srv->cfg.options, s->frame, n_slots, n_tiles, n_views, persistent, lc, nullptr,
-                    s->stream, true);
+    {
+        /* batches in flight share the GPU: plain launches (see ChainedLaunches) */
+        ChainedLaunches plain(false);
+        launch_init(s->layout, base, nullptr, nullptr, s->stream);
+        launch_pipeline(s->layout, base, srv->cfg.options, s->frame, n_slots, n_tiles, n_views, persistent, lc,
+                        nullptr, s->stream, true);
+    }
     cudaMemcpyAsync(s->h_back, base + s->layout.control_off, sizeof(Control), cudaMemcpyDeviceToHost, s->stream);
     cudaMemcpyAsync(s->h_back + sizeof(Control), base + s->layout.table_off, table_bytes, cudaMemcpyDeviceToHost,
                     s->stream);

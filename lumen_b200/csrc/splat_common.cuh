@@ -551,6 +551,19 @@ __device__ __forceinline__ void chain_begin() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+/* Whether launch_chained sets the dependent-launch attribute on this host
+ * thread (ChainedLaunches turns it off for a scope). The render server,
+ * which keeps several batches in flight on separate streams, launches
+ * without it: a chained kernel's blocks wait resident on their SMs, which
+ * would hold back the other stream's batch. */
+inline thread_local bool g_chained_launches = true;
+
+struct ChainedLaunches {
+    bool saved;
+    explicit ChainedLaunches(bool on) : saved(g_chained_launches) { g_chained_launches = on; }
+    ~ChainedLaunches() { g_chained_launches = saved; }
+};
+
 template <typename... KArgs, typename... Args>
 inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                                   Args... args) {
@@ -563,7 +576,7 @@ inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 bloc
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = g_chained_launches ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
