@@ -42,7 +42,16 @@ WIDTH, HEIGHT = 1920, 1080
 # DRAM bytes (read + write) of one composite_kernel launch at the 1 M-Gaussian
 # 1080p workload, from an ncu capture (profiles/composite_config1.md)
 COMPOSITE_DRAM_BYTES = 42.4e6
-KERNELS_PER_FRAME = 14   # init, project, 2 x (histogram + 4 digit passes), emit, tile_ranges, composite
+def kernels_per_frame(n_tiles: int) -> int:
+    """Kernels one forward frame launches: init, project, the depth sort's
+    histogram and 4 digit passes, emit, the tile sort's histogram and one
+    digit pass per byte a tile id can vary in, tile ranges, composite."""
+    tile_bytes = 0
+    t = n_tiles - 1
+    while t > 0:
+        tile_bytes += 1
+        t >>= 8
+    return 1 + 1 + (1 + 4) + 1 + (1 + tile_bytes) + 1 + 1
 
 
 def parse():
@@ -649,7 +658,7 @@ def multiview_leg(dev, steps, warmup, hbm_peak):
             "per_call_views_per_s": n_views * 1000.0 / ms_single, "per_call_ms_for_64": ms_single,
             "stages_ms": {k: round(v / steps, 4) for k, v in zip(["project", "sort", "tile_ranges", "composite"],
                                                                  stage)},
-            "visible": V, "instances": K, "tiles": T, "digit_passes": p, "gpu_launches_per_batch": 14,
+            "visible": V, "instances": K, "tiles": T, "digit_passes": p, "gpu_launches_per_batch": kernels_per_frame(T),
             "roofline": {"bytes": b, "achieved": b / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                          "frac": b / (ms * 1e-3) / 1e9 / hbm_peak}}
 
@@ -916,7 +925,7 @@ def main():
             "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": workload_config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
-            "gpu_launches": KERNELS_PER_FRAME * steps,
+            "gpu_launches": kernels_per_frame(T) * steps,
             "clocks": clk.summary(),
             "stages_ms": {n: round(v, 4) for n, v in zip(names, stage_ms)},
             "stages_timing": "a second run of the K frames with CUDA events between the stages",
