@@ -63,3 +63,19 @@ def test_sdk_mirror_heatmap_matches_the_reference_sdk_bytes(tmp_path):
     header = f"P6\n{w} {h}\n255\n".encode("ascii")
     assert raw.startswith(header)
     np.testing.assert_array_equal(np.frombuffer(raw[len(header):], np.uint8).reshape(h, w, 3), z["default"])
+
+
+def test_c_abi_argument_checks():
+    """lumen_gpu_depth_products rejects what the SDK would (host-side; nothing
+    is launched for these)."""
+    import ctypes as C
+    from lumen_b200 import _lib as L
+    lib = L.load()
+    out = L.LumenDepthProducts()
+    assert lib.lumen_gpu_depth_products(None, 4, 4, C.byref(out), None) == -1
+    assert lib.lumen_gpu_depth_products(C.c_void_p(16), 0, 4, C.byref(out), None) == -1
+    assert lib.lumen_gpu_depth_products(C.c_void_p(16), 4, 4, None, None) == -1
+    out.heatmap, out.near_plane, out.far_plane = C.c_void_p(16), 2.0, 2.0            # far == near
+    assert lib.lumen_gpu_depth_products(C.c_void_p(16), 4, 4, C.byref(out), None) == -1
+    out.heatmap = None                                                                # nothing requested
+    assert lib.lumen_gpu_depth_products(C.c_void_p(16), 4, 4, C.byref(out), None) == 0

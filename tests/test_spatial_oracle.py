@@ -106,3 +106,27 @@ def test_raycast_finds_the_nearest_valid_splat():
         assert bool(h["hit"]) == bool(ok.any())
         if ok.any():
             assert h["distance"] == pytest.approx(t[ok].min(), rel=1e-5, abs=1e-5)
+
+
+def test_c_abi_host_paths():
+    """Node counts, scratch sizes and argument checks of include/lumen_spatial.h
+    (host-side; nothing is launched)."""
+    import ctypes as C
+    from lumen_b200 import _lib as L
+    lib = L.load()
+    for n in (0, 1, 2, 3, 5, 1000, 4097, 1 << 20):
+        total, count = n, n
+        while count > 1:
+            count = (count + 1) // 2
+            total += count
+        assert lib.lumen_bvh_node_count(n) == total
+    assert lib.lumen_gpu_bvh_scratch_bytes(-1) == 0 and lib.lumen_gpu_bvh_scratch_bytes(1000) > 0
+    g, bvh = L.LumenGpuGaussians(), L.LumenGpuBvh()
+    assert lib.lumen_gpu_bvh_build(C.byref(g), C.byref(bvh), None, 0, None) == 0      # empty cloud
+    assert (bvh.leaf_count, bvh.node_count, bvh.root_index) == (0, 0, -1)
+    g.count = 10                                                                      # no arrays
+    assert lib.lumen_gpu_bvh_build(C.byref(g), C.byref(bvh), None, 0, None) == -1
+    g.count = 0
+    assert lib.lumen_gpu_raycast(C.byref(bvh), C.byref(g), None, 0, 1.0, None, None) == 0
+    g.count = 3                                                                       # hierarchy of another cloud
+    assert lib.lumen_gpu_raycast(C.byref(bvh), C.byref(g), None, 1, 1.0, None, None) == -1

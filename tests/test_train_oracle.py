@@ -119,3 +119,35 @@ def test_schedule_helpers():
     sr = lambda i: lib.lumen_training_should_reset_opacity(C.byref(c), i)
     assert [sd(i) for i in (400, 500, 550, 600, 15000, 15100)] == [0, 1, 0, 1, 1, 0]
     assert [sr(i) for i in (0, 3000, 4500, 15000, 18000)] == [0, 1, 0, 1, 0]
+
+
+def test_empty_inputs_and_argument_errors():
+    """The C ABI's host-side paths for empty clouds and bad arguments (no
+    device work is enqueued for these)."""
+    lib = L.load()
+    cfg = lib.lumen_training_default_config()
+    g = L.LumenGpuGaussians()
+    st = L.LumenAdamState()
+    assert lib.lumen_gpu_adam_step(C.byref(g), None, None, C.byref(st), C.byref(cfg), None) == 0
+    assert st.step == 1                                    # the counter advances even for an empty cloud
+    assert lib.lumen_gpu_adam_step(None, None, None, C.byref(st), C.byref(cfg), None) == -1
+    bad = lib.lumen_training_default_config()
+    bad.iterations = 0
+    assert lib.lumen_gpu_adam_step(C.byref(g), None, None, C.byref(st), C.byref(bad), None) == -1
+    g.count = 5                                            # parameters missing
+    assert lib.lumen_gpu_adam_step(C.byref(g), None, None, C.byref(st), C.byref(cfg), None) == -1
+    assert lib.lumen_gpu_accumulate_viewspace(None, 12, None, 0, 1.0, 1.0, None, None, None) == 0
+    assert lib.lumen_gpu_accumulate_viewspace(None, 1, None, 0, 1.0, 1.0, None, None, None) == -1
+    assert lib.lumen_gpu_reset_opacities(None, 0, 0.01, None) == 0
+    assert lib.lumen_gpu_reset_opacities(None, 3, 0.01, None) == -1
+    assert lib.lumen_gpu_psnr(None, None, 0, None, None, None) == -1
+    src, dst = L.LumenGpuGaussians(), L.LumenGpuGaussians()
+    stats = L.LumenDensifyStats()
+    assert lib.lumen_gpu_densify_and_prune(C.byref(src), None, None, C.byref(cfg), 1.0, C.byref(dst), None, None,
+                                           None, 0, C.byref(stats), None) == 0
+    assert dst.count == 0 and (stats.cloned, stats.split, stats.pruned, stats.count) == (0, 0, 0, 0)
+    src.count = 4                                          # output capacity below 2N
+    dst.count = 7
+    assert lib.lumen_gpu_densify_and_prune(C.byref(src), None, None, C.byref(cfg), 1.0, C.byref(dst), None, None,
+                                           None, 0, C.byref(stats), None) == -1
+    assert lib.lumen_gpu_densify_scratch_bytes(-1) == 0 and lib.lumen_gpu_densify_scratch_bytes(1000) > 0
