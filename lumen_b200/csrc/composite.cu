@@ -35,13 +35,26 @@ __device__ __forceinline__ unsigned char to_byte(float c) {
 /* A chunk of kChunk sorted instances is staged at a time. */
 template <int kChunk>
 struct CompositeSmem {
-    float4 geo[kChunk];                 /* cx, cy, depth, opacity */
-    float4 con[kChunk];                 /* 0.5 ic00, ic01, 0.5 ic11, - */
-    float4 col[kChunk];                 /* r, g, b, - */
+    float4 geo[kChunk + 1];             /* cx, cy, depth, opacity; slot kChunk: the padding splat */
+    float4 con[kChunk + 1];             /* 0.5 ic00, ic01, 0.5 ic11, - */
+    float4 col[kChunk + 1];             /* r, g, b, - */
     unsigned char mask[kChunk];         /* bit w: the splat can reach warp w's pixels */
-    unsigned short list[kTilePixels / 32][kChunk];
+    unsigned short list[kTilePixels / 32][kChunk + 4];
     unsigned int ticket;
 };
+
+/* The warp lists are padded to a multiple of four with slot kChunk, a splat
+ * whose power is above 4.5 at every pixel (conic 1e30, so it is skipped
+ * like any out-of-reach splat and changes nothing); the splat loop then
+ * runs in groups of four with one warp vote per group. */
+template <int kChunk>
+__device__ __forceinline__ void init_padding_splat(CompositeSmem<kChunk>& s) {
+    if (threadIdx.x == 0) {
+        s.geo[kChunk] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        s.con[kChunk] = make_float4(1e30f, 0.0f, 1e30f, 0.0f);
+        s.col[kChunk] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
 
 /* A pixel's front-to-back state (PixelAccumulator, compositor.mojo:10-59). */
 struct PixelState {
@@ -61,8 +74,10 @@ struct PixelState {
 template <int kChunk, bool kClamp, bool kModeAlpha>
 __device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int warp, int cnt, int cs, float pxc,
                                            float pyc, float thr, PixelState& p) {
-    for (int t = 0; t < cnt; ++t) {
-        const int j = s.list[warp][t];
+    for (int t0 = 0; t0 < cnt; t0 += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int j = s.list[warp][t0 + u];
         if (!p.done) {
             const float4 gg = s.geo[j];
             const float4 cc = s.con[j];
@@ -99,6 +114,7 @@ __device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int w
                 }
             }
         }
+    }
         if (__all_sync(0xffffffffu, p.done)) break;
     }
     if (!kModeAlpha) p.acc = 1.0f - p.T;     /* the value the reference's blend leaves (compositor.mojo:51) */
@@ -192,6 +208,8 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
                     if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned short)j;
                     cnt += __popc(bal);
                 }
+                if (lane < ((4 - (cnt & 3)) & 3)) s.list[warp][cnt + lane] = (unsigned short)kChunk;
+                cnt = (cnt + 3) & ~3;
                 __syncwarp();
                 PixelState px_state{T, cr, cg, cb, dep, acc, count, last, done};
                 if (clamp) {
@@ -242,6 +260,7 @@ composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplat
                  long long tile_offset) {
     chain_begin();
     __shared__ CompositeSmem<kChunk> s;
+    init_padding_splat(s);
     composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, tile_offset + blockIdx.x);
 }
 
@@ -253,6 +272,7 @@ composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRe
                             LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
     chain_begin();
     __shared__ CompositeSmem<kChunk> s;
+    init_padding_splat(s);
     const long long total = vt->hdr.total_tiles;
     const int n_views = vt->hdr.n_views;
     for (;;) {
