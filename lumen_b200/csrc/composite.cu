@@ -32,21 +32,29 @@ __device__ __forceinline__ unsigned char to_byte(float c) {
     return (unsigned char)(c * 255.0f);
 }
 
-/* A chunk of kChunk sorted instances is staged at a time. */
+/* A chunk of kChunk sorted instances is staged at a time; a warp walks its
+ * list of the chunk's splats kVoteGroup at a time. */
+constexpr int kVoteGroup = 8;
+
+/* Resident CTAs per SM the compositor is compiled for: 64 registers per
+ * thread, enough for the unrolled group without spills. */
+constexpr int kCompositeBlocksPerSm = 4;
+
 template <int kChunk>
 struct CompositeSmem {
     float4 geo[kChunk + 1];             /* cx, cy, depth, opacity; slot kChunk: the padding splat */
     float4 con[kChunk + 1];             /* 0.5 ic00, ic01, 0.5 ic11, - */
     float4 col[kChunk + 1];             /* r, g, b, - */
     unsigned char mask[kChunk];         /* bit w: the splat can reach warp w's pixels */
-    unsigned short list[kTilePixels / 32][kChunk + 4];
+    unsigned short list[kTilePixels / 32][kChunk + kVoteGroup];
     unsigned int ticket;
 };
 
-/* The warp lists are padded to a multiple of four with slot kChunk, a splat
- * whose power is above 4.5 at every pixel (conic 1e30, so it is skipped
- * like any out-of-reach splat and changes nothing); the splat loop then
- * runs in groups of four with one warp vote per group. */
+/* The warp lists are padded to a multiple of kVoteGroup with slot kChunk, a
+ * splat of opacity 0 whose power is above 4.5 away from (0, 0) (conic
+ * 1e30): it is skipped like any out-of-reach splat and changes nothing. The
+ * splat loop then runs in groups of kVoteGroup, unrolled, with one warp
+ * vote per group. */
 template <int kChunk>
 __device__ __forceinline__ void init_padding_splat(CompositeSmem<kChunk>& s) {
     if (threadIdx.x == 0) {
@@ -74,9 +82,9 @@ struct PixelState {
 template <int kChunk, bool kClamp, bool kModeAlpha>
 __device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int warp, int cnt, int cs, float pxc,
                                            float pyc, float thr, PixelState& p) {
-    for (int t0 = 0; t0 < cnt; t0 += 4) {
+    for (int t0 = 0; t0 < cnt; t0 += kVoteGroup) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < kVoteGroup; ++u) {
         const int j = s.list[warp][t0 + u];
         if (!p.done) {
             const float4 gg = s.geo[j];
@@ -208,8 +216,9 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
                     if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned short)j;
                     cnt += __popc(bal);
                 }
-                if (lane < ((4 - (cnt & 3)) & 3)) s.list[warp][cnt + lane] = (unsigned short)kChunk;
-                cnt = (cnt + 3) & ~3;
+                if (lane < ((kVoteGroup - (cnt & (kVoteGroup - 1))) & (kVoteGroup - 1)))
+                    s.list[warp][cnt + lane] = (unsigned short)kChunk;
+                cnt = (cnt + kVoteGroup - 1) & ~(kVoteGroup - 1);
                 __syncwarp();
                 PixelState px_state{T, cr, cg, cb, dep, acc, count, last, done};
                 if (clamp) {
@@ -254,7 +263,7 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
 
 /* One CTA per tile of the batch. */
 template <int kChunk>
-__global__ void __launch_bounds__(kTilePixels, 6)
+__global__ void __launch_bounds__(kTilePixels, kCompositeBlocksPerSm)
 composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplatRecord* __restrict__ records,
                  LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt,
                  long long tile_offset) {
@@ -267,7 +276,7 @@ composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplat
 /* Persistent form for a grid fixed in advance (a captured graph replayed
  * for batches of any size): CTAs take tiles in ticket order. */
 template <int kChunk>
-__global__ void __launch_bounds__(kTilePixels, 6)
+__global__ void __launch_bounds__(kTilePixels, kCompositeBlocksPerSm)
 composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRecord* __restrict__ records,
                             LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
     chain_begin();
@@ -290,7 +299,7 @@ static void launch_composite_chunk(const ViewTable* vt, int n_views, const Lumen
                                    const LumenRenderOptions& opt, long long tile_offset, long long n_tiles,
                                    bool persistent, int num_sms, cudaStream_t st) {
     if (persistent) {
-        launch_chained(composite_persistent_kernel<kChunk>, dim3(6 * num_sms), dim3(kTilePixels), 0, st, vt,
+        launch_chained(composite_persistent_kernel<kChunk>, dim3(kCompositeBlocksPerSm * num_sms), dim3(kTilePixels), 0, st, vt,
                        (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt);
     } else {
         launch_chained(composite_kernel<kChunk>, dim3((unsigned int)n_tiles), dim3(kTilePixels), 0, st, vt, n_views,
