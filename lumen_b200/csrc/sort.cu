@@ -140,24 +140,43 @@ struct PassSmem {
 };
 
 /* Sum over earlier tiles of digit t's count, walking back until a tile with
- * an inclusive prefix is found. */
+ * an inclusive prefix is found. The descriptors are read kLookbackWindow at
+ * a time (independent loads, one round trip per window): when every CTA
+ * starts at once, tile k's walk is about k/2 tiles long, and a walk of one
+ * load at a time made the first wave of tiles latency-bound. A descriptor
+ * not yet published stops the window; the walk resumes from it. */
+constexpr int kLookbackWindow = 4;
+
 __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, int tile, int t, unsigned int* err) {
     unsigned int excl = 0;
-    for (int j = tile - 1; j >= 0; --j) {
-        unsigned int v = 0;
-        int spins = 0;
-        for (;;) {
-            v = ld_volatile_u32(lb + (size_t)j * 256 + t);
-            if (v >> 30) break;
+    int j = tile - 1;
+    int spins = 0;
+    while (j >= 0) {
+        unsigned int d[kLookbackWindow];
+#pragma unroll
+        for (int w = 0; w < kLookbackWindow; ++w)
+            d[w] = j - w >= 0 ? ld_volatile_u32(lb + (size_t)(j - w) * 256 + t) : 0u;
+        bool done = false, stalled = false;
+#pragma unroll
+        for (int w = 0; w < kLookbackWindow; ++w) {
+            if (done || stalled) continue;
+            const unsigned int v = d[w];
+            if (!(v >> 30)) {
+                stalled = true;
+            } else {
+                excl += v & kDescMask32;
+                --j;
+                if ((v >> 30) == 2) done = true;
+            }
+        }
+        if (done) break;
+        if (stalled) {
             if (++spins >= kSpinLimit) {
                 atomicOr(err, LUMEN_GPU_ERR_SPIN_TIMEOUT);
-                v = kDescIncl32;
                 break;
             }
             __nanosleep(32);
         }
-        excl += v & kDescMask32;
-        if ((v >> 30) == 2) break;
     }
     return excl;
 }
