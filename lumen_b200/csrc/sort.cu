@@ -298,12 +298,24 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         }
         __syncthreads();
         const int nvalid = (int)((K - base) < kTileKeys ? (K - base) : kTileKeys);
-        for (int j = tid; j < nvalid; j += kSortThreads) {
-            const KeyT kk = s.keys[j];
-            const unsigned int d = (unsigned int)((kk >> shift) & 0xFF);
-            const long long out = s.gbase[d] + j;
-            kout[out] = kk;
-            vout[out] = s.vals[j];
+        if (nvalid == kTileKeys) {
+#pragma unroll
+            for (int it = 0; it < kItems; ++it) {
+                const int j = it * kSortThreads + tid;
+                const KeyT kk = s.keys[j];
+                const unsigned int d = (unsigned int)((kk >> shift) & 0xFF);
+                const long long out = s.gbase[d] + j;
+                kout[out] = kk;
+                vout[out] = s.vals[j];
+            }
+        } else {
+            for (int j = tid; j < nvalid; j += kSortThreads) {
+                const KeyT kk = s.keys[j];
+                const unsigned int d = (unsigned int)((kk >> shift) & 0xFF);
+                const long long out = s.gbase[d] + j;
+                kout[out] = kk;
+                vout[out] = s.vals[j];
+            }
         }
         __syncthreads();
     }
