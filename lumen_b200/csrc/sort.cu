@@ -13,11 +13,12 @@
  *    kernel that produced them, tell which); a pass over a constant digit
  *    leaves a stable sort unchanged, so it is skipped on the device.
  *  - each digit pass is one persistent kernel: a CTA takes 4096-key tiles in
- *    ticket order, ranks its keys with warp-level match_any multisplit over
- *    per-warp shared-memory histograms (stable: warp order, then item order,
- *    then lane order), publishes per-digit tile counts, and resolves the
- *    global digit offsets by decoupled look-back over earlier tiles. Keys
- *    are reordered in shared memory and written out in digit runs.
+ *    ticket order, counts the tile's digits and publishes the counts at
+ *    once, ranks its keys with a warp-level multisplit (one ballot per
+ *    varying bit of the digit; stable: warp order, then item order, then
+ *    lane order) straight into shared memory, and then resolves the global
+ *    digit offsets by decoupled look-back over earlier tiles. Keys are
+ *    written out in digit runs.
  *  - every wait on another CTA's descriptor is bounded.
  * Per pass and pair: (sizeof key + 4) B read and written.
  */
@@ -142,9 +143,9 @@ struct PassSmem {
 /* Sum over earlier tiles of digit t's count, walking back until a tile with
  * an inclusive prefix is found. The descriptors are read kLookbackWindow at
  * a time (independent loads, one round trip per window): when every CTA
- * starts at once, tile k's walk is about k/2 tiles long, and a walk of one
- * load at a time made the first wave of tiles latency-bound. A descriptor
- * not yet published stops the window; the walk resumes from it. */
+ * starts at once, tile k's walk is about k/2 tiles long. A descriptor not
+ * yet published stops the window; the walk resumes from it. Wider windows
+ * measured slower (more loads per step than the walks save). */
 constexpr int kLookbackWindow = 4;
 
 __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, int tile, int t, unsigned int* err) {
@@ -220,6 +221,10 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         __syncthreads();
     }
 
+    /* the bits of this digit that vary over the keys (the others are equal
+     * in every key and need no ballot) */
+    const unsigned int dbits = (unsigned int)(((sc->key_or & sc->key_or_not) >> shift) & 0xFFull);
+
     for (;;) {
         if (tid == 0) s.tile = atomicAdd(&sc->pass_ticket[digit], 1u);
         __syncthreads();
@@ -230,7 +235,6 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         /* warp w owns keys [base + w*512, +512); item i of lane l is base + w*512 + i*32 + l */
         KeyT k[kItems];
         unsigned int v[kItems];
-        unsigned short rank[kItems];
 #pragma unroll
         for (int it = 0; it < kItems; ++it) {
             const long long idx = base + warp * (kItems * 32) + it * 32 + lane;
@@ -241,19 +245,13 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         const long long wbase = base + warp * (kItems * 32);
         for (int b = lane; b < 256; b += 32) s.whist[warp][b] = 0u;
         __syncwarp();
-        /* warp-level stable multisplit */
+        /* the tile's digit counts come first (per-warp shared histograms; the
+         * order of the increments does not matter), so that the tile's
+         * aggregate is published before its keys are ranked and the
+         * look-back chain of the tiles after it moves on sooner */
 #pragma unroll
-        for (int it = 0; it < kItems; ++it) {
-            const bool valid = wbase + it * 32 + lane < K;
-            const unsigned int d = valid ? (unsigned int)((k[it] >> shift) & 0xFF) : (0x100u + lane);
-            const unsigned int peers = __match_any_sync(0xffffffffu, d);
-            unsigned int prior = 0;
-            if (valid) prior = s.whist[warp][d];
-            __syncwarp();
-            if (valid && lane == __ffs(peers) - 1) s.whist[warp][d] = prior + __popc(peers);
-            __syncwarp();
-            rank[it] = (unsigned short)(prior + __popc(peers & lanemask_lt()));
-        }
+        for (int it = 0; it < kItems; ++it)
+            if (wbase + it * 32 + lane < K) atomicAdd(&s.whist[warp][(unsigned int)((k[it] >> shift) & 0xFF)], 1u);
         __syncthreads();
         /* digit t: warp-exclusive offsets and the tile's count */
         const int t = tid;
@@ -279,23 +277,45 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
             for (int w = 0; w < warp; ++w) wb += s.warp_sums[w];
             s.digit_start[t] = wb + x - count;
         }
+        __syncthreads();
+        /* warp-level stable multisplit (warp order, then item order, then
+         * lane order): the lanes holding the same digit are found with one
+         * ballot per varying bit, a constant cost where a match instruction
+         * slows down with the number of distinct digits in the warp. The
+         * warp's running count of each digit starts at its warp-exclusive
+         * offset, so a key's rank is its place in the tile's digit run and it
+         * goes straight to its slot in shared memory. */
+#pragma unroll
+        for (int it = 0; it < kItems; ++it) {
+            const bool valid = wbase + it * 32 + lane < K;
+            const unsigned int d = (unsigned int)((k[it] >> shift) & 0xFF);
+            unsigned int peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                if (!((dbits >> b) & 1u)) continue;
+                const unsigned int bit = (d >> b) & 1u;
+                const unsigned int bal = __ballot_sync(0xffffffffu, bit);
+                peers &= bit ? bal : ~bal;
+            }
+            unsigned int prior = 0;
+            if (valid) prior = s.whist[warp][d];
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1) s.whist[warp][d] = prior + __popc(peers);
+            __syncwarp();
+            if (valid) {
+                const unsigned int pos = s.digit_start[d] + prior + __popc(peers & lanemask_lt());
+                s.keys[pos] = k[it];
+                s.vals[pos] = v[it];
+            }
+        }
+        /* the look-back runs once the keys are in shared memory (their
+         * registers are free for a wide window of descriptors) */
         unsigned int excl = 0;
         if (tile > 0) {
             excl = lookback_digit(lb, (int)tile, t, err);
             st_volatile_u32(lb + (size_t)tile * 256 + t, kDescIncl32 | (excl + count));
         }
         s.gbase[t] = (long long)s.goffset[t] + (long long)excl - (long long)s.digit_start[t];
-        __syncthreads();
-        /* reorder through shared memory */
-#pragma unroll
-        for (int it = 0; it < kItems; ++it) {
-            if (wbase + it * 32 + lane < K) {
-                const unsigned int d = (unsigned int)((k[it] >> shift) & 0xFF);
-                const unsigned int pos = s.digit_start[d] + s.whist[warp][d] + rank[it];
-                s.keys[pos] = k[it];
-                s.vals[pos] = v[it];
-            }
-        }
         __syncthreads();
         const int nvalid = (int)((K - base) < kTileKeys ? (K - base) : kTileKeys);
         if (nvalid == kTileKeys) {
