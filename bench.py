@@ -41,7 +41,7 @@ N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
 # DRAM bytes (read + write) of one composite_kernel launch at the 1 M-Gaussian
 # 1080p workload, from an ncu capture (profiles/composite_config1.md)
-COMPOSITE_DRAM_BYTES = 42.4e6
+COMPOSITE_DRAM_BYTES = 41.98e6
 def kernels_per_frame(n_tiles: int) -> int:
     """Kernels one forward frame launches: init, project, the depth sort's
     histogram and 4 digit passes, emit, the tile sort's histogram and one
