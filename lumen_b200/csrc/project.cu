@@ -169,7 +169,13 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
     }
 }
 
+/* Instances of an emission block resolved to their splats per window. */
+constexpr int kEmitWindow = 2048;
+constexpr int kEmitPerThread = kEmitWindow / kEmitThreads;
+static_assert(kEmitPerThread == 8, "two 16-byte slot groups per thread");
+
 struct EmitSmem {
+    __align__(16) unsigned int owner[kEmitWindow];   /* 1 + the block-local splat of each window slot */
     unsigned int blk;
     unsigned int warp_tot[kEmitThreads / 32];
     unsigned long long inst_base;
@@ -179,6 +185,7 @@ struct EmitSmem {
     unsigned int width[kEmitThreads];     /* tiles per rectangle row */
     unsigned int tile_base[kEmitThreads]; /* batch-wide id of the view's tile 0 */
     unsigned int tiles_x[kEmitThreads];
+    float rcp_width[kEmitThreads];        /* 1 / width, for the row of an instance */
     unsigned long long key_or, key_or_not;
 };
 
@@ -216,6 +223,7 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
             s.width[tid] = w;
             s.tile_base[tid] = (unsigned int)vd.tile_begin;
             s.tiles_x[tid] = (unsigned int)vd.tiles_x;
+            s.rcp_width[tid] = 1.0f / (float)w;
         }
         unsigned int block_inst = 0;
         const unsigned int excl = block_exclusive_scan<kEmitThreads>(cnt, s.warp_tot, &block_inst);
@@ -231,27 +239,71 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         }
         __syncthreads();
         const unsigned long long inst_base = s.inst_base;
-        unsigned long long kor = 0ull, knot = 0ull;
-        for (unsigned int j = tid; j < block_inst; j += kEmitThreads) {
-            int lo = 0, hi = kEmitThreads - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (s.incl[mid] > j) hi = mid; else lo = mid + 1;
+        unsigned int kor = 0u, knot = 0u;
+        /* The block's instances, kEmitWindow at a time. Each splat marks the
+         * slot where its run of instances enters the window (the splat
+         * already running at the window's start marks slot 0); a prefix
+         * maximum over the marks then gives every slot its splat without a
+         * search, and consecutive threads write consecutive instances. */
+        const unsigned int my_end = excl + cnt;
+        for (unsigned int a = 0; a < block_inst; a += kEmitWindow) {
+            uint4* o4 = reinterpret_cast<uint4*>(s.owner) + tid * 2;
+            o4[0] = make_uint4(0u, 0u, 0u, 0u);
+            o4[1] = make_uint4(0u, 0u, 0u, 0u);
+            __syncthreads();
+            if (cnt && my_end > a && excl < a + kEmitWindow) s.owner[(excl > a ? excl : a) - a] = (unsigned int)tid + 1u;
+            __syncthreads();
+            /* inclusive prefix maximum: eight consecutive slots per thread,
+             * then across threads */
+            const uint4 g0 = o4[0], g1 = o4[1];
+            unsigned int m[kEmitPerThread] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+            for (int k = 1; k < kEmitPerThread; ++k) m[k] = max(m[k], m[k - 1]);
+            unsigned int x = m[kEmitPerThread - 1];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x = max(x, y);
             }
-            const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
-            const unsigned int rl = s.rect_lo[lo];
-            const unsigned int min_tx = rl & 0xFFFFu, min_ty = rl >> 16;
-            const unsigned int w = s.width[lo];
-            const unsigned int q = j - start;
-            /* rows outer, columns inner (pipeline.mojo:152-153) */
-            const unsigned int tile = s.tile_base[lo] + (min_ty + q / w) * s.tiles_x[lo] + min_tx + q % w;
-            const unsigned long long pos = inst_base + j;
-            kor |= tile;
-            knot |= ~(unsigned long long)tile & 0xFFFFFFFFull;
-            if (pos < (unsigned long long)cap) {
-                f.keys[0][pos] = tile;
-                f.vals[0][pos] = s.vis[lo];
+            unsigned int pre = __shfl_up_sync(0xffffffffu, x, 1);
+            if (lane == 0) pre = 0u;
+            if (lane == 31) s.warp_tot[warp] = x;
+            __syncthreads();
+            for (int w = 0; w < warp; ++w) pre = max(pre, s.warp_tot[w]);
+            o4[0] = make_uint4(max(pre, m[0]), max(pre, m[1]), max(pre, m[2]), max(pre, m[3]));
+            o4[1] = make_uint4(max(pre, m[4]), max(pre, m[5]), max(pre, m[6]), max(pre, m[7]));
+            __syncthreads();
+            const unsigned int nwin = block_inst - a < (unsigned int)kEmitWindow ? block_inst - a : kEmitWindow;
+            for (unsigned int jj = tid; jj < nwin; jj += kEmitThreads) {
+                const int lo = (int)s.owner[jj] - 1;
+                const unsigned int j = a + jj;
+                const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
+                const unsigned int rl = s.rect_lo[lo];
+                const unsigned int min_tx = rl & 0xFFFFu, min_ty = rl >> 16;
+                const unsigned int w = s.width[lo];
+                const unsigned int q = j - start;
+                /* q / w through the reciprocal (exact after one correction
+                 * step while q < 2^20), integer division beyond */
+                unsigned int row;
+                if (q < (1u << 20)) {
+                    row = (unsigned int)((float)q * s.rcp_width[lo]);
+                    if (row * w > q) --row;
+                    else if ((row + 1u) * w <= q) ++row;
+                } else {
+                    row = q / w;
+                }
+                const unsigned int col = q - row * w;
+                /* rows outer, columns inner (pipeline.mojo:152-153) */
+                const unsigned int tile = s.tile_base[lo] + (min_ty + row) * s.tiles_x[lo] + min_tx + col;
+                const unsigned long long pos = inst_base + j;
+                kor |= tile;
+                knot |= ~tile;
+                if (pos < (unsigned long long)cap) {
+                    f.keys[0][pos] = tile;
+                    f.vals[0][pos] = s.vis[lo];
+                }
             }
+            __syncthreads();
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -259,8 +311,8 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
             knot |= __shfl_xor_sync(0xffffffffu, knot, o);
         }
         if (lane == 0 && block_inst) {
-            atomicOr(&s.key_or, kor);
-            atomicOr(&s.key_or_not, knot);
+            atomicOr(&s.key_or, (unsigned long long)kor);
+            atomicOr(&s.key_or_not, (unsigned long long)knot);
         }
         __syncthreads();
         if (tid == 0) {
