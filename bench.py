@@ -307,11 +307,16 @@ def e2e_rasterize(sc, scales, opac, steps, warmup):
         wall.append(time.perf_counter() - t0)
         gpu_ms.append(st.rasterize_time_ms)
     npix = WIDTH * HEIGHT
-    out = {"value": 1000.0 / (sum(gpu_ms) / len(gpu_ms)), "unit": UNIT,
+    wall_ms = [w * 1e3 for w in wall]
+    # the host wall clock around each call (it returns once the frame buffer
+    # is back in host memory); the library's own event time beside it
+    out = {"value": 1.0 / (sum(wall) / len(wall)), "unit": UNIT,
            "h2d_bytes_per_step": npix * 3 + npix * 4, "d2h_bytes_per_step": npix * 3 + npix * 4 + npix * 4,
            "api": "lumen_rasterize (include/lumen.h), host LumenFrameBuffer",
-           "wall_frames_per_s": 1.0 / (sum(wall) / len(wall)),
-           "p50_ms": statistics.median(gpu_ms), "p99_ms": sorted(gpu_ms)[min(len(gpu_ms) - 1, int(0.99 * len(gpu_ms)))],
+           "timing": "host wall clock per call",
+           "library_event_frames_per_s": 1000.0 / (sum(gpu_ms) / len(gpu_ms)),
+           "p50_ms": statistics.median(wall_ms),
+           "p99_ms": sorted(wall_ms)[min(len(wall_ms) - 1, int(0.99 * len(wall_ms)))],
            "visible": int(st.visible_splats), "touched_tiles": int(st.touched_tiles)}
     lib.lumen_framebuffer_destroy(fb)
     lib.lumen_rasterizer_destroy(r)
@@ -904,7 +909,7 @@ def main():
 
     stage_ms = [x / steps for x in stage]
     names = ["project", "sort", "tile_ranges", "composite"]
-    # algorithmic bytes per launch (roofline section); p = digit passes of the
+    # algorithmic bytes per launch; p = digit passes of the
     # reference's 64-bit key sort that vary (its 8-pass sort with constant digits skipped)
     P = WIDTH * HEIGHT
     p = passes

@@ -8,7 +8,7 @@ Rendering runs in liblumen.so (hand-written sm_100a CUDA behind a C ABI).
 
 Device-resident entry points: ``lumen_b200.render`` (forward with every
 stage exposed), ``lumen_b200.autograd`` (torch.autograd.Function with the
-hand-written backward), ``lumen_b200.serving`` (render server).
+hand-written backward), ``lumen_b200.serve`` (render server).
 """
 from .camera import Camera, CameraTrajectory
 from .client import LumenEngine, RasterizerConfig, RenderResult

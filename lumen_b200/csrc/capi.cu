@@ -324,6 +324,7 @@ void lumen_cloud_destroy(LumenCloud* c) {
 LumenStatus lumen_cloud_reserve(LumenCloud* c, size_t new_capacity) {
     if (!c) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (new_capacity <= c->capacity) return LUMEN_SUCCESS;
+    if (new_capacity > SIZE_MAX / sizeof(LumenGaussian)) return LUMEN_ERROR_OUT_OF_MEMORY;
     LumenGaussian* d = (LumenGaussian*)std::realloc(c->data, new_capacity * sizeof(LumenGaussian));
     if (!d) return LUMEN_ERROR_OUT_OF_MEMORY;
     c->data = d;
@@ -605,6 +606,8 @@ LumenStatus lumen_gpu_camera_from_lookat(const LumenCamera* camera, uint32_t W, 
 /* Bulk append: one copy instead of n calls (declared in lumen_gpu.h). */
 LumenStatus lumen_cloud_append(LumenCloud* c, const LumenGaussian* g, size_t n) {
     if (!c || (!g && n > 0)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    /* neither count + n nor the byte count of the copy may wrap */
+    if (n > SIZE_MAX / sizeof(LumenGaussian) - c->count) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (c->count + n > c->capacity) {
         size_t next = c->capacity * 2;
         if (next < c->count + n) next = c->count + n;

@@ -56,11 +56,21 @@ int device_sm_count() {
 
 void prime_persistent_launches();
 
-/* Kernel attributes and occupancy figures, set once per process before any
- * launch (and so before any graph capture). */
+/* Kernel attributes (the large dynamic shared memory limits) apply to the
+ * device that is current when they are set, so they are set once per
+ * device, before the first launch on it (and so before any graph capture);
+ * the occupancy figures are the same on every B200. */
+constexpr int kMaxConfiguredDevices = 64;
+
 void configure_once() {
-    static std::once_flag once;
-    std::call_once(once, [] {
+    static std::once_flag once[kMaxConfiguredDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxConfiguredDevices) {
+        configure_sort_kernels();
+        prime_persistent_launches();
+        return;
+    }
+    std::call_once(once[dev], [] {
         configure_sort_kernels();
         prime_persistent_launches();
     });

@@ -14,7 +14,8 @@
  *
  * Host code cannot use g_noalloc_scratch's name as a device address, so the
  * first call on each device (with that device current) looks the address up
- * with cudaGetSymbolAddress and caches it; that first call should come before
+ * with cudaGetSymbolAddress and caches it, and raises the digit passes'
+ * shared memory limit on that device; that first call should come before
  * any stream capture. Every call shares the array and finds the previous
  * call's contents in it: the control block is cleared on each call, and calls
  * whose work overlaps on the GPU (different streams, or different host
@@ -40,7 +41,10 @@ void configure_sort_kernels();
 namespace {
 
 constexpr long long kMaxPairs = LUMEN_GPU_NOALLOC_MAX_PAIRS;
-constexpr long long kTiles = (kMaxPairs + kSortTile - 1) / kSortTile;
+/* look-back descriptors are addressed by the 64-bit sort's tile, which the
+ * standalone scratch layout (ScratchLayout) also sizes by */
+constexpr long long kTiles = (kMaxPairs + kSort64Tile - 1) / kSort64Tile;
+static_assert(kSort64Tile == kSortTile, "the 64-bit sort's tile must be the tile the scratch layout counts");
 constexpr size_t kControlBytes = align_up(sizeof(Control), 256) + align_up(view_table_bytes(1), 256);
 /* control block and a one-view table, then 8 digit passes x tiles x 256
  * look-back descriptors */
@@ -53,10 +57,13 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes + kAltKe
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_address[kMaxDevices] = {};
+bool g_configured[kMaxDevices] = {};
 
-/* The device address of g_noalloc_scratch on the current device, looked up
- * once per device. */
-cudaError_t scratch_address(void** out) {
+/* Set-up on the current device, once per device: the device address of
+ * g_noalloc_scratch, and the digit passes' dynamic shared memory limit
+ * above 48 KB (a kernel attribute that applies to the device current when
+ * it is set; this may be the first call into the library on the device). */
+cudaError_t device_setup(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -67,6 +74,10 @@ cudaError_t scratch_address(void** out) {
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_address[dev] = p;
+    }
+    if (!g_configured[dev]) {
+        configure_sort_kernels();
+        g_configured[dev] = true;
     }
     *out = g_address[dev];
     return cudaSuccess;
@@ -97,12 +108,8 @@ extern "C" LumenStatus lumen_gpu_sort_pairs_noalloc(uint64_t* keys, uint32_t* va
     const ScratchLayout L = ScratchLayout::make(0, kMaxPairs);
     if (L.tile_lb_off != kControlBytes || L.total > kScratchBytes) return LUMEN_ERROR_INVALID_ARGUMENT;
     void* addr = nullptr;
-    cudaError_t e = scratch_address(&addr);
+    cudaError_t e = device_setup(&addr);
     if (e != cudaSuccess) return map_cuda(e);
-    /* the digit passes need more than 48 KB of dynamic shared memory; this may
-     * be the first call into the library, so allow it here too */
-    static std::once_flag configured;
-    std::call_once(configured, [] { configure_sort_kernels(); });
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char* base = (unsigned char*)addr;
     Control* ctrl = (Control*)base;

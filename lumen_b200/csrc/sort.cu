@@ -473,8 +473,8 @@ void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigne
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
                    long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
                    int num_sms, cudaStream_t st) {
-    launch_sort_impl<unsigned long long, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
-                                             8, num_sms, st);
+    launch_sort_impl<unsigned long long, kSort64Items>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr,
+                                                       nullptr, err, 8, num_sms, st);
 }
 
 void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st) {
@@ -508,8 +508,9 @@ void configure_sort_kernels() {
                          (int)sizeof(PassSmem<unsigned int, 16>));
     cudaFuncSetAttribute(onesweep_pass_kernel<unsigned int, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(PassSmem<unsigned int, 24>));
-    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned long long, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(PassSmem<unsigned long long, 16>));
+    cudaFuncSetAttribute(onesweep_pass_kernel<unsigned long long, kSort64Items>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<unsigned long long, kSort64Items>));
 }
 
 }  // namespace lumen

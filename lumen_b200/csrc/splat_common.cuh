@@ -59,6 +59,8 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;   /* 4096 keys per tile */
 constexpr int kSortTileMin = kSortThreads * 8;         /* the smallest tile a digit pass may use */
+constexpr int kSort64Items = 16;                       /* keys per thread of the 64-bit pair sort */
+constexpr int kSort64Tile = kSortThreads * kSort64Items;
 
 /* Launch parameters an autotuner may choose; none of them changes a result. */
 struct LaunchConfig {

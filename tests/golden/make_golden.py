@@ -19,7 +19,9 @@ bytes that the reference Python SDK's export_depth_visualization
 with near 1.25, far 7.5.
 
 The reference source is needed only to run this script; the tests read the
-committed files.
+committed files. Usage:
+
+    python tests/golden/make_golden.py --reference <reference checkout> [capi] [ply] [depth]
 """
 import ctypes as C
 import os
@@ -32,9 +34,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.path.join(ROOT, "oracle", "_ref", "liblumen_ref.so")
 
 
-def main():
+def main(reference: str):
     if not os.path.exists(REF):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REFERENCE={reference}"], check=True)
     lib = C.CDLL(REF)
     lib.lumen_create_synthetic_cube.restype = C.c_void_p
     lib.lumen_create_synthetic_cube.argtypes = [C.c_size_t, C.c_float]
@@ -60,10 +62,10 @@ def main():
                         **{"sphere_128_1.5": dump(lib.lumen_create_synthetic_sphere(128, 1.5))})
 
 
-def sdk_ply():
+def sdk_ply(reference: str):
     """Needs the reference source tree (its Python SDK) on this machine."""
     import sys
-    sys.path.insert(0, "/root/reference/python")
+    sys.path.insert(0, os.path.join(reference, "python"))
     from lumen.cloud import Gaussian3D, GaussianCloud
     rng = np.random.default_rng(7)
     cloud = GaussianCloud()
@@ -87,11 +89,11 @@ def sdk_ply():
                         sh=np.array([g.sh_coeffs for g in back.splats], np.float32))
 
 
-def sdk_depth_heatmap():
+def sdk_depth_heatmap(reference: str):
     """Needs the reference source tree (its Python SDK) on this machine."""
     import sys
     import tempfile
-    sys.path.insert(0, "/root/reference/python")
+    sys.path.insert(0, os.path.join(reference, "python"))
     from lumen.visualizer import export_depth_visualization
     rng = np.random.default_rng(11)
     h, w = 12, 16
@@ -113,11 +115,14 @@ def sdk_depth_heatmap():
 
 
 if __name__ == "__main__":
-    import sys
-    which = sys.argv[1:] or ["capi", "ply", "depth"]
-    if "capi" in which:
-        main()
-    if "ply" in which:
-        sdk_ply()
-    if "depth" in which:
-        sdk_depth_heatmap()
+    import argparse
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--reference", required=True, help="the reference checkout (its c_api/ and python/ trees)")
+    ap.add_argument("which", nargs="*", default=["capi", "ply", "depth"])
+    a = ap.parse_args()
+    if "capi" in a.which:
+        main(a.reference)
+    if "ply" in a.which:
+        sdk_ply(a.reference)
+    if "depth" in a.which:
+        sdk_depth_heatmap(a.reference)

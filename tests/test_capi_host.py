@@ -127,6 +127,13 @@ def test_cloud_lifecycle(lib):
     assert lib.lumen_cloud_add_gaussian(None, C.byref(g)) == -1
     arr = (L.LumenGaussian * 5)()
     assert lib.lumen_cloud_append(cloud, arr, 5) == 0 and lib.lumen_cloud_get_count(cloud) == 36
+    # counts whose sum with the current count, or whose byte size, wraps are refused before any copy
+    size_max = (1 << 64) - 1
+    for n in (size_max, size_max - 10, size_max // C.sizeof(L.LumenGaussian) - 35, 1 << 62):
+        assert lib.lumen_cloud_append(cloud, arr, n) == -1
+    assert lib.lumen_cloud_get_count(cloud) == 36
+    assert lib.lumen_cloud_reserve(cloud, size_max // 8) == -2
+    assert lib.lumen_cloud_get_capacity(cloud) < 1 << 20
     lib.lumen_cloud_clear(cloud)
     assert lib.lumen_cloud_get_count(cloud) == 0
     lib.lumen_cloud_destroy(cloud)

@@ -62,6 +62,38 @@ def test_noalloc_sort_matches_allocating_sort_twice():
         assert np.array_equal(v, order.astype(np.uint32))
 
 
+@pytest.mark.parametrize("n", [1, 4095, 4096, 4097])
+def test_noalloc_small_and_tile_edge_sizes_after_a_large_call(n):
+    """Sizes inside one 4096-key tile and at its edge, each right after a
+    full-size call, so the look-back descriptors and the alternate buffers
+    that the large call left in the shared array are there to be misread.
+    n = 1 has no varying digit: the pairs stay where the caller put them."""
+    from lumen_b200 import _lib as L
+    big_k, big_v = _case(3, 262144)
+    assert _noalloc_sort(big_k, big_v)[0] == L.LUMEN_SUCCESS
+    keys, vals = _case(10 + n, n)
+    status, k, v = _noalloc_sort(keys, vals)
+    assert status == L.LUMEN_SUCCESS
+    rk, rv = _reference_entry_point(keys, vals)
+    assert np.array_equal(k, rk) and np.array_equal(v, rv)
+    assert np.array_equal(v, np.argsort(keys, kind="stable").astype(np.uint32))
+
+
+def test_noalloc_all_equal_keys_after_a_large_call():
+    """Every key equal (no digit varies): the order is the input order."""
+    from lumen_b200 import _lib as L
+    big_k, big_v = _case(4, 200_000)
+    assert _noalloc_sort(big_k, big_v)[0] == L.LUMEN_SUCCESS
+    for n in (4097, 100_000):
+        keys = np.full(n, (7 << 32) | 12345, np.uint64)
+        vals = np.arange(n, dtype=np.uint32)[::-1].copy()
+        status, k, v = _noalloc_sort(keys, vals)
+        assert status == L.LUMEN_SUCCESS
+        assert np.array_equal(k, keys) and np.array_equal(v, vals)
+        rk, rv = _reference_entry_point(keys, vals)
+        assert np.array_equal(k, rk) and np.array_equal(v, rv)
+
+
 def test_noalloc_rejects_sizes_beyond_the_static_array():
     from lumen_b200 import _lib as L
     lib = L.load()
