@@ -356,7 +356,8 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
     img = L.LumenGpuImage()
     rgb, depth, alpha = (torch.empty((HEIGHT, WIDTH, 3), device=dev), torch.empty((HEIGHT, WIDTH), device=dev),
                          torch.empty((HEIGHT, WIDTH), device=dev))
-    img.rgb, img.depth, img.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
+    last = torch.empty((HEIGHT, WIDTH), dtype=torch.int32, device=dev)
+    img.rgb, img.depth, img.alpha, img.last_idx = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr(), last.data_ptr()
     grads = [torch.empty_like(p) for p in params]
     splat2d = torch.empty((n, 12), device=dev)
     out = L.LumenGpuGradients()
@@ -708,13 +709,76 @@ def _poisson_stream(server, ids, scene_of, cams, rate, n, pools, seed):
     return res, time.perf_counter() - t0
 
 
+def _closed_loop(server, ids, scene_of, cams, depth, n, pools):
+    """Keep `depth` requests outstanding: submit the first `depth`, then a new
+    one each time the oldest completes; returns the n results."""
+    from collections import deque
+    pending = deque()
+    res = []
+    slot_of = {k: 0 for k in pools}
+    for i in range(n):
+        if len(pending) >= depth:
+            res.append(pending.popleft().result(timeout_ms=120_000))
+        cam = cams[i]
+        key = (cam.width, cam.height)
+        out = pools[key][slot_of[key] % len(pools[key])]
+        slot_of[key] += 1
+        pending.append(server.submit(ids[scene_of[i]], cam, out=out))
+    while pending:
+        res.append(pending.popleft().result(timeout_ms=120_000))
+    return res
+
+
+def _served_summary(res, n):
+    lat = [r.latency_ms for r in res]
+    span_s = (max(r.done_ms for r in res) - min(r.submit_ms for r in res)) * 1e-3
+    return {"served_frames_per_s": n / span_s, "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
+            "mean_batch_views": sum(r.batch_views for r in res) / max(len(res), 1)}
+
+
+def _batch_ceiling(dev, dscene, lib, opt, n_views):
+    """Per-view stage costs of a batch of n_views 1080p views of one scene
+    (lumen_gpu_render_batch with stage events): projection is the only
+    stage whose input is shared by the views; the sorts, ranges and
+    compositing are per view. Returns the per-view milliseconds."""
+    from lumen_b200 import _lib as L
+    from lumen_b200 import render as R
+    from lumen_b200 import scenes
+    import torch
+    cams = scenes.orbit_cameras(n_views, WIDTH, HEIGHT, radius=10.0)
+    views = [(dscene, c) for c in cams]
+    first = R.render_batch(views, opt)
+    arr = R.batch_views(views, first.images)
+    copt = L.render_options(opt)
+    fs = first.frame.frame.c_struct()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    reps = 5
+    timer = lib.lumen_gpu_stage_timer_create(reps)
+    L.check(lib.lumen_gpu_render_batch(arr, n_views, C.byref(copt), C.byref(fs), stream), "batch")
+    for _ in range(reps):
+        L.check(lib.lumen_gpu_render_batch_timed(arr, n_views, C.byref(copt), C.byref(fs), timer, stream), "batch")
+    stage = (C.c_float * 4)()
+    total = C.c_float(0)
+    nfr = C.c_int(0)
+    L.check(lib.lumen_gpu_stage_timer_read(timer, stage, C.byref(total), C.byref(nfr)), "timer")
+    lib.lumen_gpu_stage_timer_destroy(timer)
+    per_view = {k: v / reps / n_views for k, v in zip(["project", "sort", "tile_ranges", "composite"], stage)}
+    per_view["total"] = total.value / reps / n_views
+    return per_view
+
+
 def serving_leg(dev, n_requests, hbm_budget):
-    """Render serving (configuration 4 and a 1080p stream of the 1M scene):
-    Poisson arrivals at 2000 req/s through lumen_serve (continuous batching,
-    graph launches, autotuned chunk and digit-pass tile), 8-bit RGB delivered
-    to page-locked host buffers; the same request list rendered per call
+    """Render serving (configuration 4 and a 1080p stream of the 1M scene)
+    through lumen_serve (continuous batching, graph launches, autotuned
+    chunk and digit-pass tile), 8-bit RGB delivered to page-locked host
+    buffers. One server: a warm-up that lets the autotuner time every launch
+    variant on both workloads, then tuning frozen for every timed run. Timed
+    runs: Poisson arrivals at offered rates up to and beyond capacity, and
+    closed loops holding a fixed number of requests outstanding. Latency =
+    delivery - arrival. The same request list is rendered per call
     (lumen_gpu_render_forward + copy of the 8-bit image to the host + wait,
-    one request at a time) for comparison. Latency = delivery - arrival."""
+    one request at a time) for comparison. The headline served rate is the
+    highest served frames/s of any run whose p99 is at most 20 ms."""
     import random
     import numpy as np
     import torch
@@ -735,7 +799,7 @@ def serving_leg(dev, n_requests, hbm_budget):
     res_list = scenes.SERVING_RESOLUTIONS
     orbit = {wh: scenes.orbit_cameras(64, wh[0], wh[1], radius=10.0) for wh in res_list}
     pools = {wh: [torch.empty((wh[1], wh[0], 3), dtype=torch.uint8, pin_memory=True)
-                  for _ in range(48 if wh[1] < 2000 else 24)] for wh in res_list}
+                  for _ in range(96 if wh[1] < 2000 else 48)] for wh in res_list}
 
     def workload(kind, n, seed):
         rng = random.Random(seed)
@@ -776,38 +840,61 @@ def serving_leg(dev, n_requests, hbm_budget):
             lat.append((time.perf_counter() - c0) * 1e3)
         return lat, time.perf_counter() - t0
 
+    plans = {"1080p_1M": {"rates": (1400.0, 1800.0, 2200.0, 2600.0, 3200.0), "depths": (4, 8, 16, 32, 64)},
+             "mixed": {"rates": (1400.0, 1800.0, 2200.0, 2600.0), "depths": (4, 8, 16, 32, 64)}}
     out = {}
-    for kind, rate in (("1080p_1M", 2000.0), ("1080p_1M", 1400.0), ("mixed", 2000.0), ("mixed", 1400.0)):
-        sc_of, cams = workload(kind, n_requests, seed=7 if kind == "mixed" else 8)
-        warm_of, warm_cams = workload(kind, max(n_requests // 2, 64), seed=99)
-        with serve.Server(work_budget_bytes=hbm_budget, max_views_per_batch=64, max_batches_in_flight=2,
-                          use_graphs=True, autotune=True, options=opt) as srv:
-            ids = [srv.add_scene(s) for s in dscenes]
-            _poisson_stream(srv, ids, warm_of, warm_cams, rate, len(warm_cams), pools, seed=5)   # warm-up
+    with serve.Server(work_budget_bytes=hbm_budget, max_views_per_batch=64, max_batches_in_flight=2,
+                      use_graphs=True, autotune=True, options=opt) as srv:
+        ids = [srv.add_scene(s) for s in dscenes]
+        # warm-up: every launch variant of every batch class these runs meet is timed
+        for kind in plans:
+            for rate, depth, seed in ((2000.0, None, 91), (None, 16, 92), (None, 64, 93), (1400.0, None, 94)):
+                w_of, w_cams = workload(kind, 600, seed=seed)
+                if rate:
+                    _poisson_stream(srv, ids, w_of, w_cams, rate, len(w_cams), pools, seed=seed)
+                else:
+                    _closed_loop(srv, ids, w_of, w_cams, depth, len(w_cams), pools)
+        srv.freeze_tuning(True)
+        for kind, plan in plans.items():
+            sc_of, cams = workload(kind, n_requests, seed=7 if kind == "mixed" else 8)
             s0 = srv.stats()
-            res, wall = _poisson_stream(srv, ids, sc_of, cams, rate, n_requests, pools, seed=6)
+            runs = []
+            for rate in plan["rates"]:
+                res, _ = _poisson_stream(srv, ids, sc_of, cams, rate, n_requests, pools, seed=6)
+                assert all(r.status == 0 for r in res), "served request failed"
+                runs.append(dict(mode="poisson", offered_req_per_s=rate, **_served_summary(res, n_requests)))
+            for depth in plan["depths"]:
+                res = _closed_loop(srv, ids, sc_of, cams, depth, n_requests, pools)
+                assert all(r.status == 0 for r in res), "served request failed"
+                runs.append(dict(mode="closed_loop", outstanding=depth, **_served_summary(res, n_requests)))
             s1 = srv.stats()
-        assert all(r.status == 0 for r in res), "served request failed"
-        lat = [r.latency_ms for r in res]
-        span_s = (max(r.done_ms for r in res) - min(r.submit_ms for r in res)) * 1e-3
-        # per-call: frames prepared by one untimed pass over the distinct (scene, resolution) pairs
-        per_call(sc_of[:min(len(sc_of), 64)], cams[:min(len(cams), 64)])
-        pc_lat, pc_wall = per_call(sc_of, cams)
-        batches = s1["batches"] - s0["batches"]
-        out[f"{kind}@{int(rate)}"] = {
-            "requests": n_requests, "offered_req_per_s": rate,
-            "served_frames_per_s": n_requests / span_s, "served_p50_ms": _percentile(lat, 50),
-            "served_p99_ms": _percentile(lat, 99), "mean_batch_views": n_requests / max(batches, 1),
-            "batches": batches, "requeued_batches": s1["requeued_batches"] - s0["requeued_batches"],
-            "graph_launches": s1["graph_launches"] - s0["graph_launches"],
-            "device_busy_frac": (s1["device_ms"] - s0["device_ms"]) * 1e-3 / span_s,
-            "per_call_frames_per_s": n_requests / pc_wall, "per_call_p50_ms": _percentile(pc_lat, 50),
-            "per_call_p99_ms": _percentile(pc_lat, 99),
-            "served_over_per_call": (n_requests / span_s) / (n_requests / pc_wall),
-            "launch_variants_used": sorted({(r.composite_chunk, r.sort_items) for r in res})}
-    out["workload"] = ("config 4: 8 resident scenes {50k..2M} (6.4M Gaussians), Poisson 2000 req/s, random scene, "
-                       "orbit camera and resolution in {640x480, 1280x720, 1920x1080, 3840x2160}; and a 1080p "
-                       "stream of the 1M scene; 8-bit RGB to page-locked host memory")
+            # per-call: frames prepared by one untimed pass over the distinct (scene, resolution) pairs
+            per_call(sc_of[:min(len(sc_of), 64)], cams[:min(len(cams), 64)])
+            pc_lat, pc_wall = per_call(sc_of, cams)
+            pc_fps = n_requests / pc_wall
+            ok = [r for r in runs if r["p99_ms"] is not None and r["p99_ms"] <= 20.0]
+            best = max(ok, key=lambda r: r["served_frames_per_s"]) if ok else None
+            out[kind] = {
+                "requests_per_run": n_requests, "runs": runs,
+                "per_call_frames_per_s": pc_fps, "per_call_p50_ms": _percentile(pc_lat, 50),
+                "per_call_p99_ms": _percentile(pc_lat, 99),
+                "best_served_at_p99_le_20ms": best,
+                "served_over_per_call": (best["served_frames_per_s"] / pc_fps) if best else None,
+                "batches": s1["batches"] - s0["batches"],
+                "requeued_batches": s1["requeued_batches"] - s0["requeued_batches"],
+                "explored_batches_in_timed_runs": s1["explored_batches"] - s0["explored_batches"]}
+    # the bound: what a batch of 1080p views of the 1M scene costs per view, by stage
+    ceil = _batch_ceiling(dev, dscenes[sizes.index(1_000_000)], lib, opt, 16)
+    per_view_unshared = ceil["sort"] + ceil["tile_ranges"] + ceil["composite"]
+    out["ceiling_1080p_1M"] = {
+        "per_view_stage_ms_in_16_view_batch": {k: round(v, 4) for k, v in ceil.items()},
+        "frames_per_s_if_projection_were_free": 1000.0 / per_view_unshared,
+        "frames_per_s_at_measured_batch_cost": 1000.0 / ceil["total"],
+        "note": "sorts, tile ranges and compositing read and write per-view data; only projection reads the "
+                "shared scene, so no batching can serve more than frames_per_s_if_projection_were_free"}
+    out["workload"] = ("config 4: 8 resident scenes {50k..2M} (6.4M Gaussians), random scene, orbit camera and "
+                       "resolution in {640x480, 1280x720, 1920x1080, 3840x2160}; and a 1080p stream of the 1M "
+                       "scene; 8-bit RGB to page-locked host memory; Poisson offered-rate sweep and closed loops")
     return out
 
 
@@ -959,10 +1046,9 @@ def main():
         if pg:   # replicas: the slowest rank's rate times the number of ranks
             e2e["value"] = replica_rate(e2e["value"], world, pg, dev)
         line["e2e"] = e2e
-        if "serving" in line:   # served frames against per-call renders through the drop-in C ABI
-            for k, v in line["serving"].items():
-                if k.startswith("1080p_1M"):
-                    v["served_over_capi_per_call"] = v["served_frames_per_s"] / e2e["value"]
+        srv = line.get("serving", {}).get("1080p_1M")
+        if srv and srv["best_served_at_p99_le_20ms"]:   # served frames against the drop-in C ABI per call
+            srv["served_over_capi_per_call"] = srv["best_served_at_p99_le_20ms"]["served_frames_per_s"] / e2e["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if pg:

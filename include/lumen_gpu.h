@@ -287,13 +287,14 @@ typedef struct {
 
 /* Gradients of a scalar loss L through the forward that filled `frame`
  * and `forward_image` (same gaussians, camera and options; neither reused
- * since). forward_image needs rgb and alpha (and depth when grad_depth is
- * given with compute_depth). grad_rgb [H,W,3] = dL/d rgb is required;
- * grad_depth and grad_alpha ([H,W] each) may be NULL. Per tile, each
- * pixel's splats are walked front to back with the forward's arithmetic:
- * the transmittance before every splat is recomputed (nothing per splat is
- * stored by the forward) and the colour blended behind a splat is the
- * forward's output minus the running sum. No counterpart in the reference:
+ * since). forward_image needs rgb, alpha and last_idx (and depth when
+ * grad_depth is given with compute_depth). grad_rgb [H,W,3] = dL/d rgb is
+ * required; grad_depth and grad_alpha ([H,W] each) may be NULL. Per tile,
+ * each pixel's splats are walked front to back up to its last-visited
+ * instance: the transmittance before every splat is recomputed (nothing
+ * per splat is stored by the forward), the forward's skip and clamp
+ * decisions are taken again exactly, and the colour blended behind a splat
+ * is the forward's output minus the running sum. No counterpart in the reference:
  * it has no analytic backward (src/optim/gradients.mojo:11-106 stores
  * gradients, src/optim/trainer.mojo:61-66 injects placeholders). Does not
  * wait. */

@@ -76,6 +76,7 @@ typedef struct {
     double device_ms;               /* sum of batch device times */
     int64_t slot_bytes;             /* work buffers of one slot */
     int64_t max_slots, max_tiles, max_instances, max_pixels;   /* per-batch capacities */
+    uint64_t explored_batches;      /* batches whose launch variant was an autotuner exploration */
 } LumenServeStats;
 
 /* Defaults: 8 GiB budget, 64 views, 2 batches in flight, graphs and
@@ -98,6 +99,12 @@ LumenStatus lumen_server_submit(LumenServer* server, int32_t scene, const LumenV
 LumenStatus lumen_server_wait(LumenServer* server, uint64_t request_id, double timeout_ms,
                               LumenServeResult* result);
 LumenStatus lumen_server_stats(LumenServer* server, LumenServeStats* stats);
+/* Stop (frozen = 1) or resume (0) the autotuner's exploration: while
+ * frozen, every batch uses the best launch variant timed so far for its
+ * class (or for the nearest class with timings; the configured variant when
+ * there are none) and no timing is recorded. For a measurement window
+ * after a warm-up. */
+LumenStatus lumen_server_freeze_tuning(LumenServer* server, int32_t frozen);
 
 /* The admission rule alone (host only, for tests): requests given as
  * (slots, tiles, instance estimate, pixels) in queue order; writes how many

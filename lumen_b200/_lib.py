@@ -134,7 +134,8 @@ class LumenServeStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("requeued_batches", C.c_uint64), ("rejected", C.c_uint64), ("graph_launches", C.c_uint64),
                 ("device_ms", C.c_double), ("slot_bytes", C.c_int64), ("max_slots", C.c_int64),
-                ("max_tiles", C.c_int64), ("max_instances", C.c_int64), ("max_pixels", C.c_int64)]
+                ("max_tiles", C.c_int64), ("max_instances", C.c_int64), ("max_pixels", C.c_int64),
+                ("explored_batches", C.c_uint64)]
 
 
 # ---- lumen_ply.h --------------------------------------------------------------
@@ -266,6 +267,7 @@ SIGNATURES = {
     "lumen_server_submit": (C.c_int, [_P, C.c_int32, C.POINTER(LumenViewCamera), _P, C.POINTER(C.c_uint64)]),
     "lumen_server_wait": (C.c_int, [_P, C.c_uint64, C.c_double, C.POINTER(LumenServeResult)]),
     "lumen_server_stats": (C.c_int, [_P, C.POINTER(LumenServeStats)]),
+    "lumen_server_freeze_tuning": (C.c_int, [_P, C.c_int32]),
     "lumen_serve_admit": (C.c_int32, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64), C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                       C.c_int64, C.c_int64]),

@@ -3,8 +3,8 @@
 ``render(means, log_scales, quats, opacity_logits, sh, camera, options)``
 returns (rgb [H,W,3], depth [H,W], alpha [H,W]); its backward is the
 hand-written CUDA adjoint (lumen_gpu_render_backward): per-tile
-transmittance recomputed in the backward (front to back, with the forward's
-arithmetic, from the forward's outputs), then the chain rule through the
+transmittance recomputed in the backward (front to back, up to each pixel's
+last-visited splat, from the forward's outputs), then the chain rule through the
 compositing, the conic, EWA, the projective Jacobian, Sigma = R S S^T R^T,
 the quaternion normalisation, degree-3 SH and the exp / sigmoid activations.
 It returns dL/d(means, log-scales, quats, opacity logits, SH).
@@ -39,12 +39,13 @@ class _RenderFunction(torch.autograd.Function):
         ctx.camera, ctx.options, ctx.frame = camera, opt, res.frame
         ctx.sh_shape = sh.shape
         ctx.save_for_backward(tensors[0], tensors[1], tensors[2], tensors[3].reshape(n), sh_flat, res.rgb, res.depth,
-                              res.alpha)
+                              res.alpha, res.last_idx)
+        ctx.mark_non_differentiable(res.last_idx)
         return res.rgb, res.depth, res.alpha
 
     @staticmethod
     def backward(ctx, g_rgb, g_depth, g_alpha):
-        means, log_scales, quats, logits, sh, rgb, depth, alpha = ctx.saved_tensors
+        means, log_scales, quats, logits, sh, rgb, depth, alpha, last_idx = ctx.saved_tensors
         n = means.shape[0]
         dev = means.device
         lib = L.load()
@@ -65,6 +66,7 @@ class _RenderFunction(torch.autograd.Function):
         g_alpha = g_alpha.contiguous().float() if g_alpha is not None else None
         fwd = L.LumenGpuImage()
         fwd.rgb, fwd.depth, fwd.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
+        fwd.last_idx = last_idx.data_ptr()
         L.check(lib.lumen_gpu_render_backward(C.byref(g), C.byref(cam), C.byref(opt), C.byref(fs), C.byref(fwd),
                                               g_rgb.data_ptr(),
                                               None if g_depth is None else g_depth.data_ptr(),

@@ -1,10 +1,13 @@
 """Build liblumen.so (the CUDA kernels and the C interface) in-tree for sm_100a.
 
 ``python -m lumen_b200.build`` or ``lumen_b200.build.build()``. Objects go to
-lumen_b200/_build/, the library to lumen_b200/liblumen.so. Every kernel is
-compiled with --fmad=false (no fused multiply-add contraction) so the
-projection, keys, alpha decisions and transmittance round exactly as the
-reference's operation order prescribes.
+lumen_b200/_build/, the library to lumen_b200/liblumen.so. The forward
+kernels are compiled with --fmad=false (no fused multiply-add contraction)
+so the projection, keys, alpha decisions and transmittance round exactly as
+the reference's operation order prescribes. The backward (gradients, held
+to a tolerance rather than to bits) is compiled with contraction; the
+forward decisions it repeats are written there with explicitly rounded
+operations.
 """
 from __future__ import annotations
 
@@ -22,9 +25,12 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["project.cu", "sort.cu", "composite.cu", "backward.cu", "forward.cu", "capi.cu", "noalloc.cu", "serve.cu", "ply.cu", "train.cu", "depth.cu", "spatial.cu"]
 
+# sources compiled with fused multiply-add contraction
+CONTRACTED = {"backward.cu"}
+
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+    "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
     "-I" + os.path.join(ROOT, "include"),
 ]
@@ -40,7 +46,8 @@ def _deps_mtime() -> float:
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, src.replace(".cu", ".o"))
-    cmd = [NVCC, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    fmad = "--fmad=true" if src in CONTRACTED else "--fmad=false"
+    cmd = [NVCC, *NVCC_FLAGS, fmad, "-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

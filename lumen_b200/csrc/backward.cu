@@ -4,20 +4,29 @@
  * only stores buffers, src/optim/gradients.mojo:11-106).
  *
  * K6 composite_backward_kernel: per 16x16 tile, per pixel, one front-to-
- * back sweep with the forward's own arithmetic: the transmittance T_j
- * before each splat is recomputed exactly as the forward computed it (so
- * the sweep stops on the same splat), and the colour and depth blended
- * after splat j are the forward's outputs minus the prefix sums up to j
- * (nothing per splat is stored by the forward). Per splat:
+ * back sweep over the splats the forward blended, up to the pixel's
+ * last-visited instance (the forward's last_idx output, so the sweep stops
+ * on the splat where the forward stopped). Per splat j, with the
+ * transmittance T_j before it and w_j = alpha_j T_j:
  *   dL/dc = G_rgb w, dL/dz = G_depth w,
- *   dL/dalpha = sum_ch G_ch (c_ch T_j - (C_ch - P_ch,j) / (1 - alpha))
- *             + G_depth (z T_j - (D - P_z,j) / (1 - alpha))
- *             + (G_alpha - [white] sum_ch G_ch) T_final / (1 - alpha),
- * then through alpha = min(op exp(-power), 0.99) (no gradient when clamped)
- * and power = 0.5 (a dx^2 + 2 b dx dy + c dy^2) to the centre, the conic and
- * the opacity. The 10 values per splat are reduced over the warp by
- * shuffles, over the CTA in shared memory, and added to the splat's
- * Gaussian with three vector atomics per tile.
+ *   dL/dalpha = T_j (G . col_j) - (G . C - G . P_j - g_tail) / (1 - alpha),
+ * where G . C is the upstream gradient dotted with the forward's blended
+ * colour and depth, G . P_j the same dot product of the running sum up to
+ * and including j (so G . (C - P_j) is what is blended behind j) and g_tail
+ * = (G_alpha - [white] sum_ch G_ch) T_final; then through
+ * alpha = min(op exp(-power), 0.99) (no gradient when clamped) and power =
+ * 0.5 (a dx^2 + 2 b dx dy + c dy^2) to the centre, the conic and the
+ * opacity. Gradient arithmetic uses fused multiply-adds and the hardware
+ * exponential and reciprocal; the decisions the forward took (power above
+ * 4.5, alpha below 1/255, the 0.99 clamp) are taken exactly as the forward
+ * took them: the power is formed with separately rounded operations in the
+ * forward's order, and an alpha within a few parts per million of a
+ * threshold is recomputed with the shared exponential. The 10 values per
+ * splat are summed over the warp through a shared-memory transpose (each
+ * lane writes its row; lanes 0..29 each add 11 entries of one column,
+ * three partial sums per value combine by two shuffles), over the CTA with
+ * shared atomics, and added to the splat's Gaussian with three vector
+ * atomics per tile.
  *
  * K7 project_backward_kernel: per Gaussian, the chain rule through the
  * conic inverse, the EWA product T Sigma T^T with T = J W, the projective
@@ -26,6 +35,10 @@
  * the view direction, and the exp / sigmoid activations.
  *
  * K8 l1_loss_kernel: compute_l1_loss (src/optim/loss.mojo:11-35).
+ *
+ * This file is compiled with fused multiply-add contraction; the few
+ * operations that must round as the forward's do are written with
+ * explicitly rounded intrinsics.
  */
 #include "composite_common.cuh"
 
@@ -33,15 +46,23 @@ namespace lumen {
 
 constexpr int kGrad2D = 10;   /* cx, cy, ic00, ic01, ic11, opacity, r, g, b, depth */
 constexpr int kGrad2DStride = 12;   /* floats per Gaussian in splat2d: 16-byte rows for vector atomics */
+constexpr int kBwdChunk = kTilePixels;   /* instances staged per round */
+/* per warp: 32 rows of kGrad2D values, then zero padding up to the last
+ * word a lane of the transposed read touches (31 + 30 * 10) */
+constexpr int kRedRows = 32 * kGrad2D;
+constexpr int kRedWords = 360;
+constexpr int kRedReads = 11;
 
 struct BackwardSmem {
-    float4 geo[kTilePixels];
-    float4 con[kTilePixels];
-    float4 col[kTilePixels];
-    unsigned char mask[kTilePixels];
-    unsigned short list[kTilePixels / 32][kTilePixels];
-    float acc[kTilePixels][kGrad2D];
-    unsigned int gid[kTilePixels];
+    float4 geo[kBwdChunk];        /* cx, cy, depth, opacity */
+    float4 con[kBwdChunk];        /* 0.5 ic00, ic01, 0.5 ic11, - (the forward's prescaled conic) */
+    float4 col[kBwdChunk];        /* r, g, b, - */
+    unsigned char mask[kBwdChunk];
+    unsigned short list[kTilePixels / 32][kBwdChunk];
+    float acc[kBwdChunk][kGrad2D];
+    unsigned int gid[kBwdChunk];
+    float red[kTilePixels / 32][kRedWords];
+    int tile_last;
 };
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -50,42 +71,17 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-/* Sum 16 per-lane values over the warp with 16 shuffles instead of 80: at
- * each butterfly step a lane keeps one half of its values, sends the other
- * half to its partner and adds what it receives. Afterwards lane l holds the
- * warp total of value index ((l >> 4) & 1) * 8 + ((l >> 3) & 1) * 4 +
- * ((l >> 2) & 1) * 2 + ((l >> 1) & 1) (lanes 2m and 2m+1 hold the same). */
-__device__ __forceinline__ float warp_sum16_transposed(float v[16]) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int step = 0; step < 4; ++step) {
-        const int o = 16 >> step;          /* partner distance: 16, 8, 4, 2 */
-        const int half = 8 >> step;        /* values kept: 8, 4, 2, 1 */
-        const bool upper = (lane & o) != 0;
-#pragma unroll
-        for (int i = 0; i < half; ++i) {
-            const float send = upper ? v[i] : v[i + half];
-            const float keep = upper ? v[i + half] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-        }
-    }
-    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
-}
-
-__device__ __forceinline__ int transposed_index(int lane) {
-    return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
-}
-
-/* Stage chunk [cs, cs + 256) of the tile's sorted instances: records, reach
- * masks, Gaussian ids. Returns the warp's splat list length. */
+/* Stage chunk [cs, min(cs + kBwdChunk, end)) of the tile's sorted
+ * instances: records, reach masks, Gaussian ids. Returns the warp's splat
+ * list length. */
 __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatRecord* __restrict__ records,
                                            const unsigned int* __restrict__ vals,
                                            const unsigned int* __restrict__ visible_ids, unsigned int n_visible,
-                                           Control* ctrl, int cs, int re, float tile_x0, float tile_y0) {
+                                           Control* ctrl, int cs, int end, float tile_x0, float tile_y0) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int i = cs + tid;
     unsigned int m = 0;
-    if (i < re) {
+    if (i < end) {
         const unsigned int v = vals[i];
         if (v >= n_visible) {
             atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
@@ -93,7 +89,7 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
             const float4* r4 = reinterpret_cast<const float4*>(records + v);
             const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
             s.geo[tid] = geo;
-            s.con[tid] = con;
+            s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
             s.col[tid] = __ldg(r4 + 2);
             s.gid[tid] = visible_ids[v];
             m = reach_mask(geo, con, tile_x0, tile_y0);
@@ -103,7 +99,7 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
 #pragma unroll
     for (int k = 0; k < kGrad2D; ++k) s.acc[tid][k] = 0.0f;
     __syncthreads();
-    const int n = re - cs < kTilePixels ? re - cs : kTilePixels;
+    const int n = end - cs < kBwdChunk ? end - cs : kBwdChunk;
     int cnt = 0;
     for (int base = 0; base < n; base += 32) {
         const int j = base + lane;
@@ -116,13 +112,27 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
     return cnt;
 }
 
+/* The hardware exponential of -p (p in [0, 4.5]): within a few parts per
+ * million of lumen_expf_core(-p). */
+__device__ __forceinline__ float fast_exp_neg(float p) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(p * -1.44269504088896341f));
+    return r;
+}
+
+__device__ __forceinline__ float fast_rcp(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __global__ void __launch_bounds__(kTilePixels, 4)
 composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, Control* ctrl,
                           int width, int height, int tiles_x, LumenRenderOptions opt,
                           const float* __restrict__ out_rgb, const float* __restrict__ out_depth,
-                          const float* __restrict__ out_alpha, const float* __restrict__ grad_rgb,
-                          const float* __restrict__ grad_depth, const float* __restrict__ grad_alpha,
-                          float* __restrict__ grad2d) {
+                          const float* __restrict__ out_alpha, const int* __restrict__ out_last,
+                          const float* __restrict__ grad_rgb, const float* __restrict__ grad_depth,
+                          const float* __restrict__ grad_alpha, float* __restrict__ grad2d) {
     chain_begin();
     __shared__ BackwardSmem s;
     const int tile = blockIdx.x;
@@ -135,7 +145,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     const long long cap = f.instance_capacity;
     const long long K = (long long)ctrl->n_instances < cap ? (long long)ctrl->n_instances : cap;
     if (K == 0) return;
-    int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
+    const int rs = f.ranges[2 * tile], re = f.ranges[2 * tile + 1];
     if (rs == -1 || rs >= re) return;
     if (rs < 0 || (long long)re > K) {
         if (tid == 0) atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
@@ -145,54 +155,70 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     const unsigned int* __restrict__ vals = ctrl->tile_sort.sorted_buffer ? f.vals[1] : f.vals[0];
     const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
     const float tile_x0 = (float)(tx * kTile), tile_y0 = (float)(ty * kTile);
-    const float thr = opt.term_threshold;
-    const bool mode_alpha = opt.term_mode == 1;
 
-    /* the pixel's upstream gradient and the forward's outputs: colour and
-     * depth accumulated over all blended splats, final transmittance */
-    float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, g_a = 0.0f;
-    float C_r = 0.0f, C_g = 0.0f, C_b = 0.0f, C_z = 0.0f, T_final = 1.0f;
+    /* the pixel's upstream gradient and the forward's outputs */
+    float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, Gc = 0.0f;
+    int last = -1;
+    if (tid == 0) s.tile_last = -1;
+    for (int w = kRedRows + lane; w < kRedWords; w += 32) s.red[warp][w] = 0.0f;
     if (inside) {
+        last = out_last[pix];
+        if (last >= re) {   /* self-check: a last-visited instance beyond the tile's range */
+            atomicOr(&ctrl->error_flags, LUMEN_GPU_ERR_BOUNDS);
+            last = re - 1;
+        }
         g_r = grad_rgb[pix * 3 + 0];
         g_g = grad_rgb[pix * 3 + 1];
         g_b = grad_rgb[pix * 3 + 2];
+        float C_z = 0.0f;
         if (grad_depth && opt.compute_depth) {
             g_d = grad_depth[pix];
             C_z = out_depth[pix];
         }
-        if (grad_alpha) g_a = grad_alpha[pix];
-        T_final = 1.0f - out_alpha[pix];
+        const float g_a = grad_alpha ? grad_alpha[pix] : 0.0f;
+        const float T_final = 1.0f - out_alpha[pix];
         const float bg = opt.white_background ? T_final : 0.0f;
-        C_r = out_rgb[pix * 3 + 0] - bg;
-        C_g = out_rgb[pix * 3 + 1] - bg;
-        C_b = out_rgb[pix * 3 + 2] - bg;
+        /* terms of dL/dalpha_j that scale with 1 / (1 - alpha_j) and do not
+         * change along the sweep: G . C - g_tail */
+        const float g_tail = (g_a - (opt.white_background ? (g_r + g_g + g_b) : 0.0f)) * T_final;
+        Gc = g_r * (out_rgb[pix * 3 + 0] - bg) + g_g * (out_rgb[pix * 3 + 1] - bg) +
+             g_b * (out_rgb[pix * 3 + 2] - bg) + g_d * C_z - g_tail;
     }
-    /* terms of dL/dalpha_j that scale with T_final / (1 - alpha_j) */
-    const float g_tail = (g_a - (opt.white_background ? (g_r + g_g + g_b) : 0.0f)) * T_final;
+    /* the tile's sweep ends at the last instance any of its pixels visited */
+    const int wlast = __reduce_max_sync(0xffffffffu, last);
+    __syncthreads();
+    if (lane == 0 && wlast >= rs) atomicMax(&s.tile_last, wlast);
+    __syncthreads();
+    const int end = s.tile_last + 1;   /* <= re */
+    if (end <= rs) return;
 
-    /* front to back, with the forward's own arithmetic: T and the prefix
-     * sums P are the forward's, so termination falls on the same splat, and
-     * the colour blended after splat j is C - P_j */
-    float T = 1.0f, P_r = 0.0f, P_g = 0.0f, P_b = 0.0f, P_z = 0.0f;
-    bool done = !inside;
-    for (int cs = rs; cs < re; cs += kTilePixels) {
-        if (__syncthreads_count(!done) == 0) break;
-        const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, re, tile_x0, tile_y0);
+    float T = 1.0f, GP = 0.0f;
+    float* red = s.red[warp];
+    for (int cs = rs; cs < end; cs += kBwdChunk) {
+        const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, end, tile_x0, tile_y0);
         for (int t = 0; t < cnt; ++t) {
             const int j = s.list[warp][t];
+            if (cs + j > wlast) break;   /* every pixel of the warp is past its last splat */
             float gcx = 0.0f, gcy = 0.0f, ga = 0.0f, gb = 0.0f, gc = 0.0f, gop = 0.0f;
             float gr = 0.0f, gg_ = 0.0f, gbl = 0.0f, gz = 0.0f;
             bool contrib = false;
-            if (!done) {
+            if (cs + j <= last) {
                 const float4 geo = s.geo[j], cc = s.con[j];
                 const float dx = pxc - geo.x, dy = pyc - geo.y;
-                float power = 0.5f * (cc.x * dx * dx + 2.0f * cc.y * dx * dy + cc.z * dy * dy);
-                bool skip = false, pclamp = false;
+                /* the forward's power, operation by operation */
+                float power = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(cc.x, dx), dx), __fmul_rn(__fmul_rn(cc.y, dx), dy)),
+                                        __fmul_rn(__fmul_rn(cc.z, dy), dy));
+                bool pclamp = false;
                 if (power < 0.0f) { power = 0.0f; pclamp = true; }
-                else if (power > 4.5f) skip = true;
-                if (!skip) {
-                    const float gexp = lumen_expf_core(-power);
-                    const float raw = geo.w * gexp;
+                if (!(power > 4.5f)) {
+                    float gexp = fast_exp_neg(power);
+                    float raw = geo.w * gexp;
+                    /* near the 1/255 skip or the 0.99 clamp the decision is taken
+                     * with the forward's exponential */
+                    if (fabsf(raw - min_alpha()) <= 4e-6f * min_alpha() || fabsf(raw - (float)0.99) <= 4e-6f) {
+                        gexp = lumen_expf_core(-power);
+                        raw = __fmul_rn(geo.w, gexp);
+                    }
                     const bool aclamp = raw > (float)0.99;
                     const float alpha = aclamp ? (float)0.99 : raw;
                     if (!(alpha < min_alpha())) {
@@ -203,44 +229,50 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                         gg_ = g_g * w;
                         gbl = g_b * w;
                         gz = g_d * w;
-                        P_r += col.x * w;
-                        P_g += col.y * w;
-                        P_b += col.z * w;
-                        P_z += geo.z * w;
-                        const float inv = __frcp_rn(1.0f - alpha);
-                        const float dalpha = g_r * (col.x * T - (C_r - P_r) * inv) +
-                                             g_g * (col.y * T - (C_g - P_g) * inv) +
-                                             g_b * (col.z * T - (C_b - P_b) * inv) +
-                                             g_d * (geo.z * T - (C_z - P_z) * inv) + g_tail * inv;
-                        T *= (1.0f - alpha);
-                        if (mode_alpha ? (1.0f - T >= thr) : (T <= thr)) done = true;
+                        const float gcol = g_r * col.x + g_g * col.y + g_b * col.z + g_d * geo.z;
+                        GP += w * gcol;
+                        const float one_minus = 1.0f - alpha;
+                        const float dalpha = T * gcol - (Gc - GP) * fast_rcp(one_minus);
+                        T *= one_minus;
                         if (!aclamp) {
                             gop = dalpha * gexp;
                             if (!pclamp) {
-                                const float dpower = -dalpha * geo.w * gexp;
-                                ga = 0.5f * dx * dx * dpower;
-                                gb = dx * dy * dpower;
+                                const float dpower = -gop * geo.w;
+                                const float dxp = dx * dpower;
+                                ga = 0.5f * dx * dxp;
+                                gb = dy * dxp;
                                 gc = 0.5f * dy * dy * dpower;
-                                /* d dx / d cx = -1 */
-                                gcx = -(cc.x * dx + cc.y * dy) * dpower;
-                                gcy = -(cc.y * dx + cc.z * dy) * dpower;
+                                /* d dx / d cx = -1; the staged conic holds 0.5 a and 0.5 c */
+                                gcx = -(2.0f * cc.x * dx + cc.y * dy) * dpower;
+                                gcy = -(cc.y * dx + 2.0f * cc.z * dy) * dpower;
                             }
                         }
                     }
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
-                float v[16] = {gcx, gcy, ga, gb, gc, gop, gr, gg_, gbl, gz, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                const float r = warp_sum16_transposed(v);
-                const int k = transposed_index(lane);
-                if ((lane & 1) == 0 && k < kGrad2D && r != 0.0f) atomicAdd(&s.acc[j][k], r);
+                /* warp sum by a shared-memory transpose: row `lane` holds this
+                 * lane's 10 values; lane l < 30 adds words l, l + 30, ...
+                 * (value l % 10 of rows l / 10, l / 10 + 3, ...) */
+                float2* row = reinterpret_cast<float2*>(red + lane * kGrad2D);
+                row[0] = make_float2(gcx, gcy);
+                row[1] = make_float2(ga, gb);
+                row[2] = make_float2(gc, gop);
+                row[3] = make_float2(gr, gg_);
+                row[4] = make_float2(gbl, gz);
+                __syncwarp();
+                float sum = 0.0f;
+#pragma unroll
+                for (int r = 0; r < kRedReads; ++r) sum += red[lane + 30 * r];
+                sum += __shfl_down_sync(0xffffffffu, sum, 10) + __shfl_down_sync(0xffffffffu, sum, 20);
+                if (lane < kGrad2D && sum != 0.0f) atomicAdd(&s.acc[j][lane], sum);
+                __syncwarp();
             }
-            if (__all_sync(0xffffffffu, done)) break;
         }
         __syncthreads();
         /* per (splat, tile): three vector atomics (4 + 4 + 2 values) */
         const int i = cs + tid;
-        if (i < re) {
+        if (i < end) {
             float* dst = grad2d + (size_t)s.gid[tid] * kGrad2DStride;
             const float* a = s.acc[tid];
             if (a[0] != 0.0f || a[1] != 0.0f || a[2] != 0.0f || a[3] != 0.0f)
@@ -590,7 +622,8 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenVie
                                       const float* grad_alpha, LumenGpuGradients* out, void* stream) {
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
-    if (!f || !f->scratch || !grad_rgb || !out || !fwd || !fwd->rgb || !fwd->alpha) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (!f || !f->scratch || !grad_rgb || !out || !fwd || !fwd->rgb || !fwd->alpha || !fwd->last_idx)
+        return LUMEN_ERROR_INVALID_ARGUMENT;
     if (grad_depth && opt->compute_depth && !fwd->depth) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (g->count == 0) return LUMEN_SUCCESS;
     if (!out->means || !out->scales || !out->quats || !out->opacities || !out->sh || !out->splat2d ||
@@ -605,8 +638,8 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenVie
     const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
     launch_chained(composite_backward_kernel, dim3(tiles), dim3(kTilePixels), 0, s,
                    (const LumenSplatRecord*)f->records, *f, ctrl, cam->width, cam->height, tiles_x, *opt,
-                   (const float*)fwd->rgb, (const float*)fwd->depth, (const float*)fwd->alpha, grad_rgb, grad_depth,
-                   grad_alpha, out->splat2d);
+                   (const float*)fwd->rgb, (const float*)fwd->depth, (const float*)fwd->alpha,
+                   (const int*)fwd->last_idx, grad_rgb, grad_depth, grad_alpha, out->splat2d);
     const long long nb = (g->count + 255) / 256;
     launch_chained(project_backward_kernel, dim3((unsigned int)nb), dim3(256), 0, s, *g, *cam, *opt,
                    (const int*)f->radii, (const float*)out->splat2d, *out);

@@ -26,6 +26,9 @@
 #include "splat_common.cuh"
 
 namespace lumen {
+void launch_batch_project(const ViewTable* vt, const LumenRenderOptions& opt, const LumenGpuFrame& f,
+                          Control* ctrl, unsigned long long* lb, long long n_units, bool persistent, int num_sms,
+                          cudaStream_t st);
 void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& opt, const LumenGpuFrame& f,
                     Control* ctrl, unsigned long long* lb, long long n_blocks, bool persistent, int num_sms,
                     cudaStream_t st);
@@ -161,10 +164,14 @@ __global__ void frame_init_kernel(unsigned long long* zero, long long n_words, V
 /* The frame's kernels after the view table is in place. n_slots and
  * n_tiles are the batch's (plain launches) or upper bounds (persistent
  * launches, whose kernels read the batch's sizes from the table); n_views
- * is the batch's view count, or 0 when only the table knows it. */
+ * is the batch's view count, or 0 when only the table knows it; n_units
+ * the batch's projection units (plain launches of several views). A single
+ * view is projected with its compacting scan fused in (project_kernel);
+ * several views Gaussian-major, each distinct scene read once. */
 void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRenderOptions& opt,
                      const LumenGpuFrame& f, long long n_slots, long long n_tiles, int n_views, bool persistent,
-                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite) {
+                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite,
+                     long long n_units) {
     Control* ctrl = (Control*)(base + L.control_off);
     ViewTable* vt = (ViewTable*)(base + L.table_off);
     unsigned long long* proj_lb = (unsigned long long*)(base + L.proj_lb_off);
@@ -173,7 +180,10 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
     unsigned int* tile_lb = (unsigned int*)(base + L.tile_lb_off);
     const int sms = device_sm_count();
     if (n_slots > 0) {
-        launch_project(vt, n_views, opt, f, ctrl, proj_lb, L.proj_blocks, persistent, sms, s);
+        if (n_views == 1)
+            launch_project(vt, n_views, opt, f, ctrl, proj_lb, L.proj_blocks, persistent, sms, s);
+        else
+            launch_batch_project(vt, opt, f, ctrl, proj_lb, n_units, persistent, sms, s);
         if (ev) cudaEventRecord(ev[1], s);
         launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
                       &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,
@@ -246,7 +256,7 @@ static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamer
     v.inst_begin = -1;
     if (ev) cudaEventRecord(ev[0], s);
     launch_init(L, base, &hdr, &v, s);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s, true);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s, true, 0);
     return map_cuda(cudaGetLastError());
 }
 
@@ -279,7 +289,7 @@ LumenStatus forward_banded(const LumenGpuGaussians* g, const LumenViewCamera* ca
     v.img = *img;
     v.inst_begin = -1;
     launch_init(L, base, &hdr, &v, s);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, nullptr, s, false);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, nullptr, s, false, 0);
     Control* ctrl = (Control*)(base + L.control_off);
     const ViewTable* vt = (const ViewTable*)(base + L.table_off);
     const int sms = device_sm_count();
@@ -328,6 +338,7 @@ static LumenStatus plan_batch(const LumenGpuBatchView* views, int n_views, const
     hdr->n_views = n_views;
     hdr->total_blocks = blocks;
     hdr->total_tiles = tiles;
+    if (out) hdr->total_units = assign_scene_groups(out->data(), n_views);
     return LUMEN_SUCCESS;
 }
 
@@ -354,7 +365,8 @@ static LumenStatus batch_impl(const LumenGpuBatchView* views, int n_views, const
     cudaError_t e = cudaMemcpyAsync(base + L.table_off, host.data(), host.size(), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return map_cuda(e);
     launch_init(L, base, nullptr, nullptr, s);
-    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, kDefaultLaunch, ev, s, true);
+    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, kDefaultLaunch, ev, s, true,
+                    hdr.total_units);
     return map_cuda(cudaGetLastError());
 }
 

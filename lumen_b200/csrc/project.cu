@@ -332,6 +332,238 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
     }
 }
 
+/* ---------------------------------------------------------------------
+ * Gaussian-major batch projection. Views of one scene in a batch share
+ * every input of the projection but the camera, so a unit of work is one
+ * 128-Gaussian block of a distinct scene, projected into every view of
+ * that scene: its 236 bytes per Gaussian are read once per batch instead of
+ * once per view. The visible indices stay the per-view-major order of
+ * project_kernel (view v's block b at the position the blocks before it in
+ * (view, block) order leave), so every output is the one-view-at-a-time
+ * pipeline's. Three launches:
+ *   batch_count_kernel:   per unit and view, the block's visible count
+ *                         (geometry only: 44 bytes per Gaussian);
+ *   batch_offsets_kernel: exclusive scan of the counts in (view, block)
+ *                         order (decoupled look-back over 2048-count tiles),
+ *                         written over the counts;
+ *   batch_project_kernel: per unit, the SH rows staged once, then for every
+ *                         view the full projection, the record, index,
+ *                         rectangle and depth key at the view's offset.
+ * --------------------------------------------------------------------- */
+
+constexpr int kCamWords = (int)(sizeof(DevCamera) / 4);
+static_assert(sizeof(DevCamera) % 4 == 0 && kCamWords <= kProjThreads, "camera copy layout");
+constexpr int kOffsetsThreads = 256;
+constexpr int kOffsetsItems = 8;
+constexpr int kOffsetsTile = kOffsetsThreads * kOffsetsItems;
+
+struct BatchProjSmem {
+    DevCamera cam;
+    unsigned long long unit;
+    unsigned int warp_tot[kProjThreads / 32];
+    unsigned long long key_or, key_or_not;
+};
+
+/* The counts (u32 per (view, block)) and, after them, the scan's
+ * descriptors, in the project look-back region of the scratch. */
+__device__ __forceinline__ unsigned long long* offsets_desc(unsigned long long* lb, long long total_blocks) {
+    return lb + (total_blocks + 1) / 2;
+}
+
+__device__ __forceinline__ void copy_camera(DevCamera& dst, const DevCamera& src) {
+    const int tid = threadIdx.x;
+    if (tid < kCamWords) reinterpret_cast<unsigned int*>(&dst)[tid] = reinterpret_cast<const unsigned int*>(&src)[tid];
+}
+
+/* The unit's Gaussian parameters (zeros past the scene's end). */
+struct UnitParams {
+    float mx, my, mz;
+    Prepared pr;
+};
+
+__device__ __forceinline__ UnitParams load_unit_params(const LumenGpuGaussians& g, long long i,
+                                                       const LumenRenderOptions& opt) {
+    UnitParams u;
+    u.mx = u.my = u.mz = 0.0f;
+    u.pr.ok = false;
+    u.pr.op = 0.0f;
+    u.pr.s00 = u.pr.s01 = u.pr.s02 = u.pr.s11 = u.pr.s12 = u.pr.s22 = 0.0f;
+    if (i < g.count) {
+        const float* m = g.means + i * 3;
+        const float* sc = g.scales + i * 3;
+        const float4 q = __ldg(reinterpret_cast<const float4*>(g.quats) + i);
+        u.mx = __ldg(m); u.my = __ldg(m + 1); u.mz = __ldg(m + 2);
+        u.pr = prepare_gaussian(__ldg(sc), __ldg(sc + 1), __ldg(sc + 2), Quat{q.x, q.y, q.z, q.w},
+                                __ldg(g.opacities + i), opt);
+    }
+    return u;
+}
+
+template <bool kPersistent>
+__global__ void __launch_bounds__(kProjThreads)
+batch_count_kernel(const ViewTable* __restrict__ vt, LumenRenderOptions opt, Control* ctrl,
+                   unsigned long long* lb) {
+    chain_begin();
+    __shared__ BatchProjSmem s;
+    const int tid = threadIdx.x;
+    const int n_views = vt->hdr.n_views;
+    const long long total_units = vt->hdr.total_units;
+    unsigned int* counts = reinterpret_cast<unsigned int*>(lb);
+    for (;;) {
+        if (kPersistent) {
+            if (tid == 0) s.unit = atomicAdd(&ctrl->count_ticket, 1u);
+            __syncthreads();
+        } else if (tid == 0) {
+            s.unit = blockIdx.x;
+        }
+        __syncthreads();
+        const long long u = (long long)s.unit;
+        if (u >= total_units) break;
+        const int lead = find_view_by_unit(vt, n_views, u);
+        const long long b = u - vt->view[lead].unit_begin;
+        const UnitParams up = load_unit_params(vt->view[lead].g, b * kProjThreads + tid, opt);
+        for (int v = lead; v >= 0; v = vt->view[v].group_next) {
+            copy_camera(s.cam, vt->view[v].dcam);
+            __syncthreads();
+            const bool vis = project_prepared<false>(s.cam, up.mx, up.my, up.mz, up.pr, nullptr, opt).visible;
+            const int c = __syncthreads_count(vis);
+            if (tid == 0) counts[vt->view[v].block_begin + b] = (unsigned int)c;
+        }
+        if (!kPersistent) break;
+        __syncthreads();
+    }
+}
+
+/* Exclusive scan of the (view, block) visible counts in place; the total
+ * is the batch's visible count. */
+__global__ void __launch_bounds__(kOffsetsThreads)
+batch_offsets_kernel(const ViewTable* __restrict__ vt, Control* ctrl, unsigned long long* lb) {
+    chain_begin();
+    __shared__ unsigned int warp_tot[kOffsetsThreads / 32];
+    __shared__ unsigned int tile_s;
+    __shared__ unsigned long long base_s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long nb = vt->hdr.total_blocks;
+    const long long ntiles = (nb + kOffsetsTile - 1) / kOffsetsTile;
+    unsigned int* counts = reinterpret_cast<unsigned int*>(lb);
+    unsigned long long* desc = offsets_desc(lb, nb);
+    for (;;) {
+        if (tid == 0) tile_s = atomicAdd(&ctrl->offsets_ticket, 1u);
+        __syncthreads();
+        const long long t = tile_s;
+        if (t >= ntiles) break;
+        const long long i0 = t * kOffsetsTile + (long long)tid * kOffsetsItems;
+        unsigned int c[kOffsetsItems];
+        unsigned int sum = 0;
+#pragma unroll
+        for (int k = 0; k < kOffsetsItems; ++k) {
+            c[k] = i0 + k < nb ? counts[i0 + k] : 0u;
+            sum += c[k];
+        }
+        unsigned int tot = 0;
+        const unsigned int ex = block_exclusive_scan<kOffsetsThreads>(sum, warp_tot, &tot);
+        if (tid == 0) st_volatile_u64(desc + t, (t == 0 ? kDescIncl64 : kDescAgg64) | tot);
+        if (warp == 0) {
+            const unsigned long long e = t > 0 ? lookback64(desc, (int)t, &ctrl->error_flags) : 0ull;
+            if (lane == 0) {
+                base_s = e;
+                if (t > 0) st_volatile_u64(desc + t, kDescIncl64 | (e + tot));
+            }
+        }
+        __syncthreads();
+        unsigned long long run = base_s + ex;
+#pragma unroll
+        for (int k = 0; k < kOffsetsItems; ++k) {
+            if (i0 + k < nb) counts[i0 + k] = (unsigned int)run;
+            run += c[k];
+        }
+        if (tid == 0 && t == ntiles - 1) {
+            ctrl->n_visible = (unsigned int)(base_s + tot);
+            ctrl->depth_sort.n = base_s + tot;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool kPersistent>
+__global__ void __launch_bounds__(kProjThreads)
+batch_project_kernel(const ViewTable* __restrict__ vt, LumenRenderOptions opt, LumenGpuFrame f, Control* ctrl,
+                     const unsigned long long* lb) {
+    chain_begin();
+    __shared__ BatchProjSmem s;
+    extern __shared__ float4 sh_stage[];   /* kProjThreads x 12: the unit's SH coefficients */
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int n_views = vt->hdr.n_views;
+    const long long total_units = vt->hdr.total_units;
+    const unsigned int* offsets = reinterpret_cast<const unsigned int*>(lb);
+    for (;;) {
+        if (tid == 0) {
+            s.unit = kPersistent ? (unsigned long long)atomicAdd(&ctrl->proj_ticket, 1u) : blockIdx.x;
+            s.key_or = 0ull;
+            s.key_or_not = 0ull;
+        }
+        __syncthreads();
+        const long long u = (long long)s.unit;
+        if (u >= total_units) break;
+        const int lead = find_view_by_unit(vt, n_views, u);
+        const LumenGpuGaussians& g = vt->view[lead].g;
+        const long long b = u - vt->view[lead].unit_begin;
+        const long long i0 = b * kProjThreads, i = i0 + tid;
+        {
+            const long long count = g.count;
+            const int nblk = (int)(count - i0 < kProjThreads ? count - i0 : kProjThreads);
+            const float4* src = reinterpret_cast<const float4*>(g.sh + i0 * 48);
+            for (int c = tid; c < nblk * 12; c += kProjThreads) cp_async16(sh_stage + c, src + c);
+            cp_async_commit();
+        }
+        const UnitParams up = load_unit_params(g, i, opt);
+        const bool in_scene = i < g.count;
+        cp_async_wait_all();
+        unsigned long long kor = 0ull, knot = 0ull;
+        for (int v = lead; v >= 0; v = vt->view[v].group_next) {
+            copy_camera(s.cam, vt->view[v].dcam);
+            __syncthreads();
+            const Projected p = project_prepared<true>(s.cam, up.mx, up.my, up.mz, up.pr,
+                                                       reinterpret_cast<const float*>(sh_stage + tid * 12), opt);
+            const long long blk = vt->view[v].block_begin + b;
+            if (f.radii && in_scene) f.radii[blk * kProjThreads + tid] = p.visible ? p.radius : 0;
+            unsigned int n_vis = 0;
+            const unsigned int vis_local = block_exclusive_scan<kProjThreads>(p.visible ? 1u : 0u, s.warp_tot, &n_vis);
+            if (p.visible) {
+                const unsigned long long vid = (unsigned long long)offsets[blk] + vis_local;
+                float4* dst = reinterpret_cast<float4*>(f.records + vid);
+                dst[0] = make_float4(p.cx, p.cy, p.z, p.op);
+                dst[1] = make_float4(p.ic00, p.ic01, p.ic11, 0.0f);
+                dst[2] = make_float4(p.r, p.g, p.b, 0.0f);
+                f.visible_ids[vid] = (unsigned int)i;
+                f.rects[vid] = pack_rect(p.min_tx, p.min_ty, p.max_tx, p.max_ty, v);
+                const unsigned int dk = depth_key(p.z, opt.key_mode);
+                f.depth_keys[0][vid] = dk;
+                f.depth_order[0][vid] = (unsigned int)vid;
+                kor |= dk;
+                knot |= ~(unsigned long long)dk & 0xFFFFFFFFull;
+            }
+            __syncthreads();   /* s.cam and s.warp_tot are rewritten for the next view */
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+            knot |= __shfl_xor_sync(0xffffffffu, knot, o);
+        }
+        if (lane == 0 && (kor | knot)) {
+            atomicOr(&s.key_or, kor);
+            atomicOr(&s.key_or_not, knot);
+        }
+        __syncthreads();
+        if (tid == 0 && (s.key_or | s.key_or_not)) {
+            atomicOr(&ctrl->depth_sort.key_or, s.key_or);
+            atomicOr(&ctrl->depth_sort.key_or_not, s.key_or_not);
+        }
+        if (!kPersistent) break;
+        __syncthreads();
+    }
+}
+
 static int resident_ctas(const void* kernel, int threads, size_t smem) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm <= 0)
@@ -339,7 +571,7 @@ static int resident_ctas(const void* kernel, int threads, size_t smem) {
     return per_sm;
 }
 
-static int g_project_per_sm = 0, g_emit_per_sm = 0;
+static int g_project_per_sm = 0, g_emit_per_sm = 0, g_batch_count_per_sm = 0, g_batch_project_per_sm = 0;
 constexpr size_t kProjStageBytes = (size_t)kProjThreads * 48 * sizeof(float);
 
 /* Kernel attributes and the occupancy of the persistent kernels, set and
@@ -349,6 +581,37 @@ void prime_persistent_launches() {
     cudaFuncSetAttribute(project_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kProjStageBytes);
     g_project_per_sm = resident_ctas((const void*)project_kernel<true>, kProjThreads, kProjStageBytes);
     g_emit_per_sm = resident_ctas((const void*)emit_kernel<true>, kEmitThreads, 0);
+    cudaFuncSetAttribute(batch_project_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kProjStageBytes);
+    cudaFuncSetAttribute(batch_project_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kProjStageBytes);
+    g_batch_count_per_sm = resident_ctas((const void*)batch_count_kernel<true>, kProjThreads, 0);
+    g_batch_project_per_sm = resident_ctas((const void*)batch_project_kernel<true>, kProjThreads, kProjStageBytes);
+}
+
+/* Gaussian-major projection of a batch: n_units is the batch's unit count
+ * (plain launches: one CTA per unit) or 0 for persistent launches, which
+ * read the count from the table. */
+void launch_batch_project(const ViewTable* vt, const LumenRenderOptions& opt, const LumenGpuFrame& f,
+                          Control* ctrl, unsigned long long* lb, long long n_units, bool persistent, int num_sms,
+                          cudaStream_t st) {
+    if (persistent) {
+        const int pc = g_batch_count_per_sm > 0 ? g_batch_count_per_sm : 1;
+        launch_chained(batch_count_kernel<true>, dim3(pc * num_sms), dim3(kProjThreads), 0, st, vt, opt, ctrl, lb);
+    } else {
+        if (n_units <= 0) return;
+        launch_chained(batch_count_kernel<false>, dim3((unsigned int)n_units), dim3(kProjThreads), 0, st, vt, opt,
+                       ctrl, lb);
+    }
+    launch_chained(batch_offsets_kernel, dim3(2 * num_sms), dim3(kOffsetsThreads), 0, st, vt, ctrl, lb);
+    if (persistent) {
+        const int pp = g_batch_project_per_sm > 0 ? g_batch_project_per_sm : 1;
+        launch_chained(batch_project_kernel<true>, dim3(pp * num_sms), dim3(kProjThreads), kProjStageBytes, st, vt,
+                       opt, f, ctrl, (const unsigned long long*)lb);
+    } else {
+        launch_chained(batch_project_kernel<false>, dim3((unsigned int)n_units), dim3(kProjThreads), kProjStageBytes,
+                       st, vt, opt, f, ctrl, (const unsigned long long*)lb);
+    }
 }
 
 /* Plain launches: one CTA per block (n_blocks known on the host).

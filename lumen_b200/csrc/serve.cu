@@ -41,7 +41,8 @@ void launch_init(const ScratchLayout& L, unsigned char* base, const BatchHeader*
                  cudaStream_t s);
 void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRenderOptions& opt,
                      const LumenGpuFrame& f, long long n_slots, long long n_tiles, int n_views, bool persistent,
-                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite);
+                     const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite,
+                     long long n_units);
 
 namespace {
 
@@ -107,21 +108,44 @@ struct Slot {
 
 /* Per batch class (log2 of pixels, log2 of instances), the mean device time
  * per instance of each variant; explores each variant kExplore times, then
- * uses the best, re-trying all every kRefresh batches of the class. */
+ * uses the best, re-trying all every kRefresh batches of the class. While
+ * frozen it explores nothing: a class uses its best variant so far, or the
+ * best of the nearest class that has timings, or the fallback. */
 struct Tuner {
     static constexpr int kExplore = 2, kRefresh = 256;
     struct Klass { int tries[kVariants] = {}; double cost[kVariants] = {}; int batches = 0; };
     std::map<int, Klass> classes;
-    int pick(int klass) {
-        Klass& c = classes[klass];
-        const int round = c.batches % kRefresh;
-        if (round < kExplore * kVariants) return round % kVariants;
-        int best = 0;
-        for (int v = 1; v < kVariants; ++v)
-            if (c.tries[v] && (c.tries[best] == 0 || c.cost[v] / c.tries[v] < c.cost[best] / c.tries[best])) best = v;
+    bool frozen = false;
+    static int best_of(const Klass& c) {
+        int best = -1;
+        for (int v = 0; v < kVariants; ++v)
+            if (c.tries[v] && (best < 0 || c.cost[v] / c.tries[v] < c.cost[best] / c.tries[best])) best = v;
         return best;
     }
+    /* the variant for a batch of the class; *exploring tells whether it is
+     * an exploratory pick */
+    int pick(int klass, int fallback, bool* exploring) {
+        *exploring = false;
+        if (frozen) {
+            int best = -1, dist = 1 << 30;
+            for (const auto& kv : classes) {
+                const int b = best_of(kv.second);
+                const int d = std::abs(kv.first - klass);
+                if (b >= 0 && d < dist) { best = b; dist = d; }
+            }
+            return best >= 0 ? best : fallback;
+        }
+        Klass& c = classes[klass];
+        const int round = c.batches % kRefresh;
+        if (round < kExplore * kVariants) {
+            *exploring = true;
+            return round % kVariants;
+        }
+        const int best = best_of(c);
+        return best >= 0 ? best : fallback;
+    }
     void record(int klass, int variant, double cost) {
+        if (frozen) return;
         Klass& c = classes[klass];
         c.batches++;
         if (c.batches % kRefresh == 1) {   /* a new exploration round forgets old timings */
@@ -231,7 +255,7 @@ cudaError_t alloc_slot(LumenServer* srv, Slot* s) {
 
 /* The batch's work on the slot's stream, up to the counter read-back. */
 void enqueue_batch_work(LumenServer* srv, Slot* s, const LaunchConfig& lc, bool persistent, long long n_slots,
-                        long long n_tiles, int n_views, size_t table_bytes) {
+                        long long n_tiles, int n_views, size_t table_bytes, long long n_units) {
     unsigned char* base = (unsigned char*)s->frame.scratch;
     cudaMemcpyAsync(base + s->layout.table_off, s->h_table, table_bytes, cudaMemcpyHostToDevice, s->stream);
     {
@@ -239,7 +263,7 @@ void enqueue_batch_work(LumenServer* srv, Slot* s, const LaunchConfig& lc, bool 
         ChainedLaunches plain(false);
         launch_init(s->layout, base, nullptr, nullptr, s->stream);
         launch_pipeline(s->layout, base, srv->cfg.options, s->frame, n_slots, n_tiles, n_views, persistent, lc,
-                        nullptr, s->stream, true);
+                        nullptr, s->stream, true, n_units);
     }
     cudaMemcpyAsync(s->h_back, base + s->layout.control_off, sizeof(Control), cudaMemcpyDeviceToHost, s->stream);
     cudaMemcpyAsync(s->h_back + sizeof(Control), base + s->layout.table_off, table_bytes, cudaMemcpyDeviceToHost,
@@ -251,7 +275,7 @@ cudaError_t capture(LumenServer* srv, Slot* s, int variant) {
     cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     enqueue_batch_work(srv, s, kVariantTable[variant], true, srv->max_slots, srv->max_tiles, 0,
-                       view_table_bytes(srv->cfg.max_views_per_batch));
+                       view_table_bytes(srv->cfg.max_views_per_batch), 0);
     e = cudaStreamEndCapture(s->stream, &g);
     if (e != cudaSuccess) return e;
     e = cudaGraphInstantiate(&s->exec[variant], g, 0);
@@ -260,8 +284,9 @@ cudaError_t capture(LumenServer* srv, Slot* s, int variant) {
 }
 
 /* Fill the slot's page-locked view table for its batch; returns the
- * batch's projection slots and tiles. */
-void build_table(LumenServer* srv, Slot* s, long long* n_slots, long long* n_tiles) {
+ * batch's projection slots, tiles and projection units (views of one scene
+ * share their units). */
+void build_table(LumenServer* srv, Slot* s, long long* n_slots, long long* n_tiles, long long* n_units) {
     ViewTable* vt = (ViewTable*)s->h_table;
     long long blocks = 0, tiles = 0, pix = 0;
     const int nv = (int)s->batch.size();
@@ -284,15 +309,17 @@ void build_table(LumenServer* srv, Slot* s, long long* n_slots, long long* n_til
     vt->hdr.n_views = nv;
     vt->hdr.total_blocks = blocks;
     vt->hdr.total_tiles = tiles;
+    vt->hdr.total_units = assign_scene_groups(vt->view, nv);
     *n_slots = blocks * kProjThreads;
     *n_tiles = tiles;
+    *n_units = vt->hdr.total_units;
 }
 
 /* Scheduler-thread side of a launch (no lock held). */
 cudaError_t launch_batch(LumenServer* srv, Slot* s) {
     cudaSetDevice(srv->device);
-    long long n_slots = 0, n_tiles = 0;
-    build_table(srv, s, &n_slots, &n_tiles);
+    long long n_slots = 0, n_tiles = 0, n_units = 0;
+    build_table(srv, s, &n_slots, &n_tiles, &n_units);
     const LaunchConfig lc = kVariantTable[s->variant];
     cudaError_t e = cudaEventRecord(s->ev_start, s->stream);
     if (e != cudaSuccess) return e;
@@ -301,7 +328,7 @@ cudaError_t launch_batch(LumenServer* srv, Slot* s) {
         if ((e = cudaGraphLaunch(s->exec[s->variant], s->stream)) != cudaSuccess) return e;
     } else {
         enqueue_batch_work(srv, s, lc, false, n_slots, n_tiles, (int)s->batch.size(),
-                           view_table_bytes((int)s->batch.size()));
+                           view_table_bytes((int)s->batch.size()), n_units);
     }
     long long pix = 0;
     for (const ReqPtr& r : s->batch) {
@@ -369,8 +396,10 @@ void scheduler_main(LumenServer* srv) {
         int64_t inst = 0, pix = 0;
         for (const ReqPtr& r : s->batch) { inst += r->inst_est; pix += r->pixels; }
         s->klass = log2_bucket(pix) * 64 + log2_bucket(inst);
-        s->variant = srv->cfg.autotune ? srv->tuner.pick(s->klass)
-                                       : std::max(0, variant_of(srv->cfg.composite_chunk, srv->cfg.sort_items));
+        const int fixed = std::max(0, variant_of(srv->cfg.composite_chunk, srv->cfg.sort_items));
+        bool exploring = false;
+        s->variant = srv->cfg.autotune ? srv->tuner.pick(s->klass, fixed, &exploring) : fixed;
+        if (exploring) srv->stats.explored_batches++;
         const double t = now_ms(srv->t0);
         for (const ReqPtr& r : s->batch) {
             r->result.start_ms = t;
@@ -608,6 +637,13 @@ LumenStatus lumen_server_wait(LumenServer* srv, uint64_t id, double timeout_ms, 
     }
     *result = r->result;
     srv->requests.erase(id);
+    return LUMEN_SUCCESS;
+}
+
+LumenStatus lumen_server_freeze_tuning(LumenServer* srv, int32_t frozen) {
+    if (!srv) return LUMEN_ERROR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->tuner.frozen = frozen != 0;
     return LUMEN_SUCCESS;
 }
 

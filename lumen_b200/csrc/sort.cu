@@ -343,7 +343,12 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
 
 /* binning.mojo:51-73 in parallel, on tile-sorted 32-bit tile ids: a tile's
  * range starts where its id first appears and ends after it last appears.
- * Empty tiles keep the (-1, -1) the histogram kernel wrote. */
+ * Empty tiles keep the (-1, -1) the histogram kernel wrote.
+ *
+ * Each lane takes 4 consecutive ids per round (one 16-byte load; the
+ * frame's key buffers are 16-byte aligned), its neighbours' ids come from
+ * the adjacent lanes, and a group of four equal ids between equal
+ * neighbours (almost every group) is done after one comparison chain. */
 __global__ void __launch_bounds__(256)
 tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, ViewTable* vt,
                    int* ranges, Control* ctrl) {
@@ -353,21 +358,28 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
     const int n_views = vt->hdr.n_views;
     const long long K = sort_count(sc, capacity);
     const unsigned int* __restrict__ keys = sc->sorted_buffer ? k1 : k0;
+    const int lane = threadIdx.x & 31;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     unsigned int touched = 0;
-    /* each thread takes 4 consecutive keys per iteration (one 16-byte load
-     * when aligned) and compares each with its neighbours */
-    for (long long i0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4; i0 < K; i0 += nthreads * 4) {
+    /* the warp's first id, so that the loop and its shuffles are warp-uniform */
+    for (long long wb = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4; wb < K; wb += nthreads * 4) {
+        const long long i0 = wb + 4 * lane;
         unsigned int k[4];
         if (i0 + 3 < K) {
             const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
             k[0] = q.x; k[1] = q.y; k[2] = q.z; k[3] = q.w;
         } else {
 #pragma unroll
-            for (int r = 0; r < 4; ++r) k[r] = i0 + r < K ? keys[i0 + r] : 0u;
+            for (int r = 0; r < 4; ++r) k[r] = i0 + r < K ? keys[i0 + r] : 0xFFFFFFFFu;
         }
-        const unsigned int prev = i0 > 0 ? keys[i0 - 1] : 0xFFFFFFFFu;
-        const unsigned int next = i0 + 4 < K ? keys[i0 + 4] : 0xFFFFFFFFu;
+        const unsigned int up = __shfl_up_sync(0xffffffffu, k[3], 1);
+        const unsigned int down = __shfl_down_sync(0xffffffffu, k[0], 1);
+        if (i0 >= K) continue;
+        const unsigned int prev = lane > 0 ? up : (i0 > 0 ? keys[i0 - 1] : 0xFFFFFFFFu);
+        const unsigned int next = lane < 31 ? down : (i0 + 4 < K ? keys[i0 + 4] : 0xFFFFFFFFu);
+        if (i0 > 0 && i0 + 4 < K && prev == k[0] && k[0] == k[1] && k[1] == k[2] && k[2] == k[3] && k[3] == next &&
+            (long long)k[0] < n_tiles)
+            continue;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const long long i = i0 + r;
@@ -378,7 +390,7 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
                 continue;
             }
             const unsigned int before = r == 0 ? prev : k[r - 1];
-            const unsigned int after = (r == 3 || i + 1 >= K) ? (i + 1 >= K ? 0xFFFFFFFFu : next) : k[r + 1];
+            const unsigned int after = r == 3 ? next : k[r + 1];   /* 0xFFFFFFFF past the end */
             if (i == 0 || before != t) {
                 ranges[2 * (size_t)t] = (int)i;
                 ++touched;
@@ -391,7 +403,7 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) touched += __shfl_xor_sync(0xffffffffu, touched, o);
-    if ((threadIdx.x & 31) == 0 && touched) atomicAdd(&ctrl->touched_tiles, touched);
+    if (lane == 0 && touched) atomicAdd(&ctrl->touched_tiles, touched);
 }
 
 /* OR and OR-of-complement of n keys and the pair count, for sorts whose

@@ -14,6 +14,8 @@
 #pragma once
 
 #include <stdint.h>
+#include <map>
+#include <tuple>
 #include <cuda_runtime.h>
 
 #include "../../include/lumen_gpu.h"
@@ -48,7 +50,9 @@ struct Control {
     unsigned int error_flags;            /* LUMEN_GPU_ERR_* */
     unsigned int touched_tiles;
     unsigned int composite_ticket;       /* tile order of the compositor */
-    unsigned int pad[8];
+    unsigned int count_ticket;           /* unit order of the batch visibility count */
+    unsigned int offsets_ticket;         /* tile order of the batch offset scan */
+    unsigned int pad[6];
     SortControl depth_sort;              /* visible splats by depth key */
     SortControl tile_sort;               /* instances by tile id */
 };
@@ -105,6 +109,11 @@ struct ViewDesc {
     long long tile_begin;
     long long inst_begin;     /* first tile-sorted instance of the view, or -1
                                  (written on the device by the range pass) */
+    long long unit_begin;     /* batch projection: the first unit of the view's scene group
+                                 when the view leads the group (units of the views before it
+                                 otherwise, so the view owns none) */
+    int group_next;           /* the next view of the same scene, or -1 */
+    int group_lead;           /* 1: the first view of its scene in the batch */
     DevCamera dcam;           /* derived from cam on the device before projection */
 };
 
@@ -113,7 +122,7 @@ struct BatchHeader {
     int reserved0;
     long long total_blocks;   /* projection blocks of all views */
     long long total_tiles;    /* tiles of all views */
-    long long reserved1;
+    long long total_units;    /* batch projection: blocks of the batch's distinct scenes */
 };
 
 /* Header and views, in scratch; written before the frame's kernels run. */
@@ -154,6 +163,32 @@ struct ScratchLayout {
     size_t zeroed_prefix() const { return table_off; }
 };
 
+/* Groups a batch's views by scene (identical LumenGpuGaussians) for the
+ * Gaussian-major batch projection: each view's group_next and group_lead,
+ * and the unit numbering (one unit per 128-Gaussian block of each distinct
+ * scene, in order of the scenes' first views). Returns the unit count. */
+inline long long assign_scene_groups(ViewDesc* v, int n) {
+    using Key = std::tuple<const void*, const void*, const void*, const void*, const void*, long long>;
+    std::map<Key, int> last;   /* the latest view of each scene so far */
+    long long units = 0;
+    for (int i = 0; i < n; ++i) {
+        const LumenGpuGaussians& g = v[i].g;
+        const Key key{g.means, g.scales, g.quats, g.opacities, g.sh, (long long)g.count};
+        v[i].group_next = -1;
+        auto it = last.find(key);
+        v[i].group_lead = it == last.end() ? 1 : 0;
+        if (it != last.end()) {
+            v[it->second].group_next = i;
+            it->second = i;
+        } else {
+            last.emplace(key, i);
+        }
+        v[i].unit_begin = units;
+        if (v[i].group_lead) units += (g.count + kProjThreads - 1) / kProjThreads;
+    }
+    return units;
+}
+
 /* Tile rectangle of a visible splat and its view: 12 bits per bound (tile
  * coordinates below 4096, images up to 65520 pixels a side), view in the
  * top 16 bits. */
@@ -178,6 +213,16 @@ __device__ __forceinline__ int find_view_by_block(const ViewTable* vt, int n_vie
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (vt->view[mid].block_begin <= blk) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+/* The scene group that owns batch projection unit u: the last view with
+ * unit_begin <= u (non-leading views own no units). */
+__device__ __forceinline__ int find_view_by_unit(const ViewTable* vt, int n_views, long long u) {
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (vt->view[mid].unit_begin <= u) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -337,20 +382,55 @@ __device__ __forceinline__ void sh_color(const float* __restrict__ sh, float dx0
     r = rr; g = gg; b = bb;
 }
 
-/* One Gaussian: cull, camera transform, EWA, radius, tile rectangle, colour.
- * Follows pipeline.mojo:85-149 and the functions it calls. */
-__device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, float mx, float my, float mz,
-                                                      float sx, float sy, float sz, Quat qraw, float op,
-                                                      const float* __restrict__ sh, const LumenRenderOptions& o) {
-    Projected p;
-    p.visible = false;
-    p.radius = 0;
+/* The view-independent part of a Gaussian's projection: activations, the
+ * normalised rotation, the opacity cull and Sigma = M M^T with M = R(q) S
+ * (gaussian.mojo:36-44, culling.mojo:47-51, covariance.mojo:41-83). */
+struct Prepared {
+    float op;
+    float s00, s01, s02, s11, s12, s22;
+    bool ok;                 /* passed the opacity cull */
+};
+
+__device__ __forceinline__ Prepared prepare_gaussian(float sx, float sy, float sz, Quat qraw, float op,
+                                                     const LumenRenderOptions& o) {
+    Prepared pr;
     if (o.params_are_logits) {
         sx = lumen_expf(sx); sy = lumen_expf(sy); sz = lumen_expf(sz);
         op = 1.0f / (1.0f + lumen_expf(-op));                 /* gaussian.mojo:43-44 */
     }
     Quat rot = q_normalized(qraw);                            /* gaussian.mojo:36 */
-    if (!(op >= min_alpha())) return p;                       /* culling.mojo:47-51 */
+    pr.op = op;
+    pr.ok = op >= min_alpha();                                /* culling.mojo:47-51 */
+    /* Covariance3D.from_scale_and_rotation, covariance.mojo:41-83 */
+    if (sx < (float)0.00001) sx = (float)0.00001;
+    if (sy < (float)0.00001) sy = (float)0.00001;
+    if (sz < (float)0.00001) sz = (float)0.00001;
+    float R[9];
+    q_to_matrix(rot, R);
+    float m00 = R[0] * sx, m01 = R[1] * sy, m02 = R[2] * sz;
+    float m10 = R[3] * sx, m11 = R[4] * sy, m12 = R[5] * sz;
+    float m20 = R[6] * sx, m21 = R[7] * sy, m22 = R[8] * sz;
+    pr.s00 = m00 * m00 + m01 * m01 + m02 * m02;
+    pr.s01 = m00 * m10 + m01 * m11 + m02 * m12;
+    pr.s02 = m00 * m20 + m01 * m21 + m02 * m22;
+    pr.s11 = m10 * m10 + m11 * m11 + m12 * m12;
+    pr.s12 = m10 * m20 + m11 * m21 + m12 * m22;
+    pr.s22 = m20 * m20 + m21 * m21 + m22 * m22;
+    return pr;
+}
+
+/* The per-view part: camera transform and cull, screen position, EWA,
+ * radius, tile rectangle, colour (kFull; without it only the visibility,
+ * radius and rectangle are formed, with the same arithmetic). Follows
+ * pipeline.mojo:85-149 and the functions it calls. */
+template <bool kFull = true>
+__device__ __forceinline__ Projected project_prepared(const DevCamera& cam, float mx, float my, float mz,
+                                                      const Prepared& pr, const float* __restrict__ sh,
+                                                      const LumenRenderOptions& o) {
+    Projected p;
+    p.visible = false;
+    p.radius = 0;
+    if (!pr.ok) return p;
     /* world_to_cam, camera.mojo:69-71, quaternion.mojo:80-87 */
     float rx = mx - cam.px, ry = my - cam.py, rz = mz - cam.pz;
     Quat t = q_mul(cam.qi, Quat{0.0f, rx, ry, rz});
@@ -362,21 +442,6 @@ __device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, floa
     if (tzs < (float)0.0001 && tzs > (float)-0.0001) tzs = (float)0.0001;
     float u = cam.fx * (tx / tzs) + cam.cx;
     float v = cam.fy * (ty / tzs) + cam.cy;
-    /* Covariance3D.from_scale_and_rotation, covariance.mojo:41-83 */
-    if (sx < (float)0.00001) sx = (float)0.00001;
-    if (sy < (float)0.00001) sy = (float)0.00001;
-    if (sz < (float)0.00001) sz = (float)0.00001;
-    float R[9];
-    q_to_matrix(rot, R);
-    float m00 = R[0] * sx, m01 = R[1] * sy, m02 = R[2] * sz;
-    float m10 = R[3] * sx, m11 = R[4] * sy, m12 = R[5] * sz;
-    float m20 = R[6] * sx, m21 = R[7] * sy, m22 = R[8] * sz;
-    float s00 = m00 * m00 + m01 * m01 + m02 * m02;
-    float s01 = m00 * m10 + m01 * m11 + m02 * m12;
-    float s02 = m00 * m20 + m01 * m21 + m02 * m22;
-    float s11 = m10 * m10 + m11 * m11 + m12 * m12;
-    float s12 = m10 * m20 + m11 * m21 + m12 * m22;
-    float s22 = m20 * m20 + m21 * m21 + m22 * m22;
     /* ProjectiveJacobian.compute, projection.mojo:80-96 */
     float jz = tz;
     if (jz < (float)0.0001) jz = (float)0.0001;
@@ -392,12 +457,12 @@ __device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, floa
     float t10 = j11 * W[3] + j12 * W[6];
     float t11 = j11 * W[4] + j12 * W[7];
     float t12 = j11 * W[5] + j12 * W[8];
-    float q00 = t00 * s00 + t01 * s01 + t02 * s02;
-    float q01 = t00 * s01 + t01 * s11 + t02 * s12;
-    float q02 = t00 * s02 + t01 * s12 + t02 * s22;
-    float q10 = t10 * s00 + t11 * s01 + t12 * s02;
-    float q11 = t10 * s01 + t11 * s11 + t12 * s12;
-    float q12 = t10 * s02 + t11 * s12 + t12 * s22;
+    float q00 = t00 * pr.s00 + t01 * pr.s01 + t02 * pr.s02;
+    float q01 = t00 * pr.s01 + t01 * pr.s11 + t02 * pr.s12;
+    float q02 = t00 * pr.s02 + t01 * pr.s12 + t02 * pr.s22;
+    float q10 = t10 * pr.s00 + t11 * pr.s01 + t12 * pr.s02;
+    float q11 = t10 * pr.s01 + t11 * pr.s11 + t12 * pr.s12;
+    float q12 = t10 * pr.s02 + t11 * pr.s12 + t12 * pr.s22;
     float c00 = q00 * t00 + q01 * t01 + q02 * t02 + o.lowpass;
     float c01 = q00 * t10 + q01 * t11 + q02 * t12;
     float c11 = q10 * t10 + q11 * t11 + q12 * t12 + o.lowpass;
@@ -424,6 +489,9 @@ __device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, floa
     if (max_py >= cam.height) max_py = cam.height - 1;
     p.min_tx = (int)(min_px / kTile); p.max_tx = (int)(max_px / kTile);
     p.min_ty = (int)(min_py / kTile); p.max_ty = (int)(max_py / kTile);
+    p.radius = radius > 0x7FFFFFFFll ? 0x7FFFFFFF : (int)radius;
+    p.visible = true;
+    if (!kFull) return p;
     /* view direction (vector.mojo:106-110) and colour, pipeline.mojo:133-139 */
     float vx = mx - cam.px, vy = my - cam.py, vz = mz - cam.pz;
     float vl = sqrtf(vx * vx + vy * vy + vz * vz);
@@ -440,10 +508,16 @@ __device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, floa
         p.ic01 = -c01 * inv_det;
         p.ic11 = c00 * inv_det;
     }
-    p.cx = u; p.cy = v; p.z = tz; p.op = op;
-    p.radius = radius > 0x7FFFFFFFll ? 0x7FFFFFFF : (int)radius;
-    p.visible = true;
+    p.cx = u; p.cy = v; p.z = tz; p.op = pr.op;
     return p;
+}
+
+/* One Gaussian: cull, camera transform, EWA, radius, tile rectangle, colour.
+ * Follows pipeline.mojo:85-149 and the functions it calls. */
+__device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, float mx, float my, float mz,
+                                                      float sx, float sy, float sz, Quat qraw, float op,
+                                                      const float* __restrict__ sh, const LumenRenderOptions& o) {
+    return project_prepared<true>(cam, mx, my, mz, prepare_gaussian(sx, sy, sz, qraw, op, o), sh, o);
 }
 
 /* float_to_ordered_uint32 (radix_sort.mojo:8-18) or the raw float bits. */

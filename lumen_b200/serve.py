@@ -97,6 +97,11 @@ class Server:
         return ServeResult(request.out, int(r.status), int(r.batch_views), float(r.submit_ms), float(r.start_ms),
                            float(r.done_ms), int(r.n_instances), int(r.composite_chunk), int(r.sort_items))
 
+    def freeze_tuning(self, frozen: bool = True) -> None:
+        """Stop (or resume) the autotuner's exploration: while frozen every
+        batch runs the best launch variant timed so far for its class."""
+        L.check(self._lib.lumen_server_freeze_tuning(self._h, int(bool(frozen))), "server_freeze_tuning")
+
     def stats(self) -> dict:
         s = L.LumenServeStats()
         L.check(self._lib.lumen_server_stats(self._h, C.byref(s)), "server_stats")

@@ -96,7 +96,8 @@ class Trainer:
     def _images(self, h: int, w: int):
         if self.image is None or self.image[0].shape[:2] != (h, w):
             e = lambda *s: torch.empty(s, dtype=torch.float32, device=self.dev)
-            self.image = (e(h, w, 3), e(h, w), e(h, w), e(h, w, 3))        # rgb, depth, alpha, dL/drgb
+            self.image = (e(h, w, 3), e(h, w), e(h, w), e(h, w, 3),        # rgb, depth, alpha, dL/drgb,
+                          torch.empty((h, w), dtype=torch.int32, device=self.dev))   # last-visited splat
         return self.image
 
     def train_step(self, camera: ViewCamera, ground_truth: torch.Tensor, iteration: int) -> TrainingMetrics:
@@ -113,11 +114,12 @@ class Trainer:
         H, W = int(camera.height), int(camera.width)
         if gt.numel() != H * W * 3:
             raise L.LumenError(-1, "train_step: ground truth does not match the camera's image size")
-        rgb, depth, alpha, gimg = self._images(H, W)
+        rgb, depth, alpha, gimg, last = self._images(H, W)
         g = self._gaussians()
         cam, opt = L.view_camera(camera), L.render_options(self.options)
         img = L.LumenGpuImage()
         img.rgb, img.depth, img.alpha = rgb.data_ptr(), depth.data_ptr(), alpha.data_ptr()
+        img.last_idx = last.data_ptr()
         out = L.LumenGpuGradients()
         out.means, out.scales, out.quats, out.opacities, out.sh = (t.data_ptr() for t in self.grads)
         out.splat2d = self.splat2d.data_ptr()

@@ -173,3 +173,26 @@ def test_request_too_large_for_a_slot_is_rejected():
         st = srv.stats()
     assert r.status == -2 and st["rejected"] == 1     # LUMEN_ERROR_OUT_OF_MEMORY
     assert ok.status == 0
+
+
+def test_frozen_tuning_explores_nothing_and_images_unchanged(world):
+    """After a warm-up in which the autotuner explores, freezing it stops
+    every exploratory pick (the stats counter stays put) and the served
+    images still equal their alone-renders."""
+    from lumen_b200 import serve
+    sc, reqs, refs = world
+    with serve.Server(work_budget_bytes=1 << 30, max_views_per_batch=8, max_batches_in_flight=2,
+                      use_graphs=True, autotune=True, options=OPT) as srv:
+        serve_all(srv, sc, reqs)
+        warm = srv.stats()
+        assert warm["explored_batches"] > 0
+        srv.freeze_tuning(True)
+        ids = list(range(len(sc)))
+        res = [srv.submit(ids[s], c) for s, c in reqs]
+        out = [h.result(timeout_ms=60_000) for h in res]
+        after = srv.stats()
+        assert after["explored_batches"] == warm["explored_batches"]
+        assert after["batches"] > warm["batches"]
+        for r, ref in zip(out, refs):
+            assert r.status == 0 and torch.equal(r.image, ref)
+        srv.freeze_tuning(False)
