@@ -398,6 +398,23 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
     b1.record()
     torch.cuda.synchronize(dev)
     bwd_ms = b0.elapsed_time(b1) / max(steps // 4, 1)
+    # stage split of the backward and of this workload's forward (a second,
+    # event-instrumented run)
+    reps = max(min(steps, 20), 1)
+    timer = lib.lumen_gpu_stage_timer_create(reps)
+    for _ in range(reps):
+        L.check(lib.lumen_gpu_render_backward_timed(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs), C.byref(img),
+                                                    gimg.data_ptr(), None, None, C.byref(out), timer, stream),
+                "backward_timed")
+    bst = (C.c_float * 4)()
+    btot, nfr = C.c_float(0), C.c_int(0)
+    L.check(lib.lumen_gpu_stage_timer_read(timer, bst, C.byref(btot), C.byref(nfr)), "timer")
+    for _ in range(reps):
+        L.check(lib.lumen_gpu_render_forward_timed(C.byref(g), C.byref(ccam), C.byref(copt), C.byref(fs),
+                                                   C.byref(img), timer, stream), "forward_timed")
+    fst = (C.c_float * 4)()
+    L.check(lib.lumen_gpu_stage_timer_read(timer, fst, C.byref(btot), C.byref(nfr)), "timer")
+    lib.lumen_gpu_stage_timer_destroy(timer)
     # the public API: torch.autograd with the same step
     leaves = [p.clone().requires_grad_(True) for p in params]
     ta_steps = max(steps // 4, 3)
@@ -412,8 +429,13 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
     b_fwd = 244 * n + 64 * V + (68 + 24 * passes) * K + 8 * T + 16 * P
     b_bwd = 80 * K + 12 * P + 88 * V + 472 * n
     total = b_fwd + 24 * P + b_bwd
+    stages = {"project": fst[0] / reps, "sort": fst[1] / reps, "tile_ranges": fst[2] / reps,
+              "composite": fst[3] / reps, "composite_backward": bst[0] / reps, "project_backward": bst[1] / reps}
     return {"workload": "config 3: 500k Gaussians, 1920x1080, L1 to the perturbed-scene render",
             "steps_per_s": 1000.0 / ms, "ms_per_step": ms, "backward_ms": bwd_ms,
+            "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+            "stages_timing": "a second, event-instrumented run of the forward and of the backward",
+            "sizes": {"n": n, "visible": V, "instances": K, "pixels": P, "tiles": T, "digit_passes": passes},
             "autograd_api_steps_per_s": 1000.0 / api_ms, "visible": V, "instances": K,
             "roofline": {"bytes": total, "achieved": total / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                          "frac": total / (ms * 1e-3) / 1e9 / hbm_peak}}
@@ -898,6 +920,67 @@ def serving_leg(dev, n_requests, hbm_budget):
     return out
 
 
+def ncu_counters():
+    """Per-kernel counters of the latest ncu captures (profiles/kernel_counters.csv:
+    one row per kernel and workload, with the command that captured it)."""
+    import csv
+    path = os.path.join(ROOT, "profiles", "kernel_counters.csv")
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        rows = [r for r in csv.DictReader(l for l in f if not l.startswith("#"))]
+    for r in rows:
+        for k in list(r):
+            try:
+                r[k] = float(r[k]) if k not in ("stage", "kernel", "workload", "binding", "capture") else r[k]
+            except (TypeError, ValueError):
+                pass
+    return rows
+
+
+def kernels_table(line, hbm_peak):
+    """Each stage of the forward (configuration 1) and of the backward
+    (configuration 3): live CUDA-event milliseconds, algorithmic bytes and
+    their fraction of the HBM peak, and the instruction-issue and pipe
+    figures of its kernels from the latest ncu capture. A stage whose
+    kernels are issue-bound reports that as its bound."""
+    counters = ncu_counters()
+    rows = []
+
+    def add(stage, workload, ms, bytes_):
+        gbs = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
+        ncu = [{k: v for k, v in c.items() if k not in ("stage", "workload")} for c in counters
+               if c.get("stage") == stage and c.get("workload") == workload]
+        binding = None
+        if ncu:
+            top = max(ncu, key=lambda c: c.get("duration_us") or 0)
+            binding = top.get("binding")
+        rows.append({"stage": stage, "workload": workload, "ms": round(ms, 4), "algorithmic_bytes": int(bytes_),
+                     "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak if gbs else None, "binding": binding,
+                     "ncu": ncu})
+
+    c = line.get("counts", {})
+    st = line.get("stages_ms", {})
+    N, V, K, T, p = N_GAUSSIANS, c.get("visible", 0), c.get("instances", 0), c.get("tiles", 0), c.get("digit_passes", 0)
+    P = WIDTH * HEIGHT
+    if st:
+        add("project", "config 1", st["project"], 236 * N + 48 * V + 4 * N)
+        add("sort", "config 1", st["sort"], 8 * N + 16 * V + 12 * K + 8 * K + 24 * K * p)
+        add("tile_ranges", "config 1", st["tile_ranges"], 8 * K + 8 * T)
+        add("composite", "config 1", st["composite"], 40 * K + 16 * P)
+    fb = line.get("fwd_bwd")
+    if fb and "stages_ms" in fb:
+        z, s3 = fb["sizes"], fb["stages_ms"]
+        n3, V3, K3, P3, T3, p3 = z["n"], z["visible"], z["instances"], z["pixels"], z["tiles"], z["digit_passes"]
+        add("project", "config 3", s3["project"], 236 * n3 + 48 * V3 + 4 * n3)
+        add("sort", "config 3", s3["sort"], 8 * n3 + 16 * V3 + 12 * K3 + 8 * K3 + 24 * K3 * p3)
+        add("tile_ranges", "config 3", s3["tile_ranges"], 8 * K3 + 8 * T3)
+        add("composite", "config 3", s3["composite"], 40 * K3 + 16 * P3)
+        add("composite_backward", "config 3", s3["composite_backward"], 80 * K3 + 12 * P3)
+        add("project_backward", "config 3", s3["project_backward"], 88 * V3 + 472 * n3)
+    return rows
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -1049,6 +1132,7 @@ def main():
         srv = line.get("serving", {}).get("1080p_1M")
         if srv and srv["best_served_at_p99_le_20ms"]:   # served frames against the drop-in C ABI per call
             srv["served_over_capi_per_call"] = srv["best_served_at_p99_le_20ms"]["served_frames_per_s"] / e2e["value"]
+    line["kernels"] = kernels_table(line, hbm_peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if pg:

@@ -303,6 +303,15 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* gaussians, const 
                                       const LumenGpuImage* forward_image, const float* grad_rgb,
                                       const float* grad_depth, const float* grad_alpha, LumenGpuGradients* grads,
                                       void* stream);
+/* lumen_gpu_render_backward with CUDA events on its stream for the timer's
+ * next frame (see lumen_gpu_stage_timer_create): stage 0 = the compositing
+ * adjoint (with the clearing of splat2d), stage 1 = the projection
+ * adjoint, stages 2 and 3 empty. No counterpart in the reference. */
+LumenStatus lumen_gpu_render_backward_timed(const LumenGpuGaussians* gaussians, const LumenViewCamera* camera,
+                                            const LumenRenderOptions* options, const LumenGpuFrame* frame,
+                                            const LumenGpuImage* forward_image, const float* grad_rgb,
+                                            const float* grad_depth, const float* grad_alpha,
+                                            LumenGpuGradients* grads, LumenGpuStageTimer* timer, void* stream);
 
 /* Mean L1 loss and its subgradient, compute_l1_loss (src/optim/loss.mojo:11-35):
  * loss = mean |pred - target|, grad[i] = +1/n if pred[i] - target[i] >= 0

@@ -234,6 +234,10 @@ SIGNATURES = {
                                             C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame),
                                             C.POINTER(LumenGpuImage), _P, _P, _P, C.POINTER(LumenGpuGradients),
                                             _P]),
+    "lumen_gpu_render_backward_timed": (C.c_int, [C.POINTER(LumenGpuGaussians), C.POINTER(LumenViewCamera),
+                                                  C.POINTER(LumenRenderOptions), C.POINTER(LumenGpuFrame),
+                                                  C.POINTER(LumenGpuImage), _P, _P, _P,
+                                                  C.POINTER(LumenGpuGradients), _P, _P]),
     "lumen_gpu_l1_loss_scratch_bytes": (C.c_size_t, []),
     "lumen_gpu_l1_loss": (C.c_int, [_P, _P, C.c_int64, _P, _P, _P, _P]),
     "lumen_gpu_camera_from_lookat": (C.c_int, [C.POINTER(LumenCamera), C.c_uint32, C.c_uint32, C.c_float,

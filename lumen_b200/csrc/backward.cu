@@ -46,24 +46,26 @@ namespace lumen {
 
 constexpr int kGrad2D = 10;   /* cx, cy, ic00, ic01, ic11, opacity, r, g, b, depth */
 constexpr int kGrad2DStride = 12;   /* floats per Gaussian in splat2d: 16-byte rows for vector atomics */
-constexpr int kBwdChunk = kTilePixels;   /* instances staged per round */
-/* per warp: 32 rows of kGrad2D values, then zero padding up to the last
- * word a lane of the transposed read touches (31 + 30 * 10) */
-constexpr int kRedRows = 32 * kGrad2D;
-constexpr int kRedWords = 360;
-constexpr int kRedReads = 11;
+constexpr int kBwdChunk = kTilePixels;   /* instances staged per round (list entries fit a byte) */
+static_assert(kBwdChunk <= 256, "warp lists hold byte offsets");
+/* Warp sums are formed for three splats at a time: lane l writes its 10
+ * values of splat u to row l, columns 10 u .. 10 u + 9 of a 32 x 30 buffer;
+ * lane c < 30 then adds column c (value c % 10 of splat c / 10). */
+constexpr int kRedSplats = 3;
+constexpr int kRedCols = kRedSplats * kGrad2D;
+constexpr int kRedWords = 32 * kRedCols;
 
 struct BackwardSmem {
     float4 geo[kBwdChunk];        /* cx, cy, depth, opacity */
     float4 con[kBwdChunk];        /* 0.5 ic00, ic01, 0.5 ic11, - (the forward's prescaled conic) */
     float4 col[kBwdChunk];        /* r, g, b, - */
     unsigned char mask[kBwdChunk];
-    unsigned short list[kTilePixels / 32][kBwdChunk];
+    unsigned char list[kTilePixels / 32][kBwdChunk];
     float acc[kBwdChunk][kGrad2D];
-    unsigned int gid[kBwdChunk];
     float red[kTilePixels / 32][kRedWords];
     int tile_last;
 };
+constexpr size_t kBwdSmemBytes = sizeof(BackwardSmem);
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
@@ -91,7 +93,6 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
             s.geo[tid] = geo;
             s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
             s.col[tid] = __ldg(r4 + 2);
-            s.gid[tid] = visible_ids[v];
             m = reach_mask(geo, con, tile_x0, tile_y0);
         }
     }
@@ -105,11 +106,33 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
         const int j = base + lane;
         const bool bit = j < n && ((s.mask[j] >> warp) & 1u);
         const unsigned int bal = __ballot_sync(0xffffffffu, bit);
-        if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned short)j;
+        if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned char)j;
         cnt += __popc(bal);
     }
     __syncwarp();
     return cnt;
+}
+
+/* The buffered splats' warp sums (n of them, columns 10 u .. 10 u + 9 of
+ * splat u), added to the CTA's accumulators. */
+__device__ __forceinline__ void flush_warp_sums(BackwardSmem& s, const float* red, int n, int j0, int j1, int j2) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < kGrad2D * n) {
+        float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+        for (int r = 0; r < 32; r += 4) {
+            a0 += red[kRedCols * r + lane];
+            a1 += red[kRedCols * (r + 1) + lane];
+            a2 += red[kRedCols * (r + 2) + lane];
+            a3 += red[kRedCols * (r + 3) + lane];
+        }
+        const float sum = (a0 + a1) + (a2 + a3);
+        const int u = lane >= 2 * kGrad2D ? 2 : lane >= kGrad2D ? 1 : 0;
+        const int j = u == 0 ? j0 : u == 1 ? j1 : j2;
+        if (sum != 0.0f) atomicAdd(&s.acc[j][lane - kGrad2D * u], sum);
+    }
+    __syncwarp();
 }
 
 /* The hardware exponential of -p (p in [0, 4.5]): within a few parts per
@@ -134,7 +157,8 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                           const float* __restrict__ grad_rgb, const float* __restrict__ grad_depth,
                           const float* __restrict__ grad_alpha, float* __restrict__ grad2d) {
     chain_begin();
-    __shared__ BackwardSmem s;
+    extern __shared__ __align__(16) unsigned char bwd_smem[];
+    BackwardSmem& s = *reinterpret_cast<BackwardSmem*>(bwd_smem);
     const int tile = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
@@ -160,7 +184,6 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, Gc = 0.0f;
     int last = -1;
     if (tid == 0) s.tile_last = -1;
-    for (int w = kRedRows + lane; w < kRedWords; w += 32) s.red[warp][w] = 0.0f;
     if (inside) {
         last = out_last[pix];
         if (last >= re) {   /* self-check: a last-visited instance beyond the tile's range */
@@ -196,6 +219,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     float* red = s.red[warp];
     for (int cs = rs; cs < end; cs += kBwdChunk) {
         const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, end, tile_x0, tile_y0);
+        int nbuf = 0, j0 = 0, j1 = 0, j2 = 0;   /* splats buffered for the warp sums (warp-uniform) */
         for (int t = 0; t < cnt; ++t) {
             const int j = s.list[warp][t];
             if (cs + j > wlast) break;   /* every pixel of the warp is past its last splat */
@@ -251,29 +275,26 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
-                /* warp sum by a shared-memory transpose: row `lane` holds this
-                 * lane's 10 values; lane l < 30 adds words l, l + 30, ...
-                 * (value l % 10 of rows l / 10, l / 10 + 3, ...) */
-                float2* row = reinterpret_cast<float2*>(red + lane * kGrad2D);
+                float2* row = reinterpret_cast<float2*>(red + lane * kRedCols + kGrad2D * nbuf);
                 row[0] = make_float2(gcx, gcy);
                 row[1] = make_float2(ga, gb);
                 row[2] = make_float2(gc, gop);
                 row[3] = make_float2(gr, gg_);
                 row[4] = make_float2(gbl, gz);
-                __syncwarp();
-                float sum = 0.0f;
-#pragma unroll
-                for (int r = 0; r < kRedReads; ++r) sum += red[lane + 30 * r];
-                sum += __shfl_down_sync(0xffffffffu, sum, 10) + __shfl_down_sync(0xffffffffu, sum, 20);
-                if (lane < kGrad2D && sum != 0.0f) atomicAdd(&s.acc[j][lane], sum);
-                __syncwarp();
+                if (nbuf == 0) j0 = j; else if (nbuf == 1) j1 = j; else j2 = j;
+                if (++nbuf == kRedSplats) {
+                    flush_warp_sums(s, red, nbuf, j0, j1, j2);
+                    nbuf = 0;
+                }
             }
         }
+        if (nbuf) flush_warp_sums(s, red, nbuf, j0, j1, j2);
         __syncthreads();
         /* per (splat, tile): three vector atomics (4 + 4 + 2 values) */
         const int i = cs + tid;
-        if (i < end) {
-            float* dst = grad2d + (size_t)s.gid[tid] * kGrad2DStride;
+        const unsigned int v = i < end ? vals[i] : n_visible;
+        if (v < n_visible) {
+            float* dst = grad2d + (size_t)f.visible_ids[v] * kGrad2DStride;
             const float* a = s.acc[tid];
             if (a[0] != 0.0f || a[1] != 0.0f || a[2] != 0.0f || a[3] != 0.0f)
                 atomicAdd(reinterpret_cast<float4*>(dst), make_float4(a[0], a[1], a[2], a[3]));
@@ -331,30 +352,18 @@ __device__ __forceinline__ void sh_term(int k, float x, float y, float z, float&
     }
 }
 
-__global__ void __launch_bounds__(256, 3)
-project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt,
-                        const int* __restrict__ radii, const float* __restrict__ grad2d, LumenGpuGradients out) {
-    chain_begin();
-    __shared__ DevCamera cam_s;
-    if (threadIdx.x == 0) setup_camera(camera, cam_s);
-    __syncthreads();
-    const DevCamera& cam = cam_s;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.count) return;
+constexpr int kProjBwdThreads = 128;
+constexpr size_t kProjBwdStageBytes = (size_t)kProjBwdThreads * 48 * sizeof(float);
+
+/* One visible Gaussian's gradients. row: its 48 SH coefficients staged in
+ * shared memory (chunk q at q ^ swz), overwritten with dL/dsh. */
+__device__ __forceinline__ void project_backward_gaussian(const LumenGpuGaussians& g, const DevCamera& cam,
+                                                          const LumenRenderOptions& opt, long long i,
+                                                          const float* __restrict__ grad2d,
+                                                          const LumenGpuGradients& out, float4* row, int swz) {
     float* gm = out.means + i * 3;
     float* gs = out.scales + i * 3;
     float* gq = out.quats + i * 4;
-    float* gsh = out.sh + i * 48;
-    if (radii[i] <= 0) {
-        gm[0] = gm[1] = gm[2] = 0.0f;
-        gs[0] = gs[1] = gs[2] = 0.0f;
-        gq[0] = gq[1] = gq[2] = gq[3] = 0.0f;
-        out.opacities[i] = 0.0f;
-        float4* gsh4 = reinterpret_cast<float4*>(gsh);
-#pragma unroll
-        for (int k = 0; k < 12; ++k) gsh4[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        return;
-    }
     const float4 G0 = reinterpret_cast<const float4*>(grad2d + i * kGrad2DStride)[0];
     const float4 G1 = reinterpret_cast<const float4*>(grad2d + i * kGrad2DStride)[1];
     const float2 G2 = reinterpret_cast<const float2*>(grad2d + i * kGrad2DStride)[4];
@@ -455,7 +464,6 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
         const bool dok = len > (float)0.000001;
         const float dx_ = dok ? vx / len : 0.0f, dy_ = dok ? vy / len : 0.0f, dz_ = dok ? vz / len : 0.0f;
         const int n = opt.sh_degree == 0 ? 1 : opt.sh_degree == 1 ? 4 : opt.sh_degree == 2 ? 9 : 16;
-        const float4* sh4 = reinterpret_cast<const float4*>(g.sh + i * 48);
         /* two streaming passes over the coefficients, 4 at a time (12 floats
          * = 3 float4): the colour before the clamp (which channels pass a
          * gradient), then the direction gradient and dL/dsh */
@@ -463,7 +471,7 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
 #pragma unroll
         for (int grp = 0; grp < 4; ++grp) {
             if (4 * grp >= n) break;
-            const float4 a = __ldg(sh4 + 3 * grp), b = __ldg(sh4 + 3 * grp + 1), c = __ldg(sh4 + 3 * grp + 2);
+            const float4 a = row[(3 * grp) ^ swz], b = row[(3 * grp + 1) ^ swz], c = row[(3 * grp + 2) ^ swz];
             const float e[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
@@ -481,12 +489,11 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
         const float gc1 = (v1 < 0.0f || v1 > 1.0f) ? 0.0f : g_col[1];
         const float gc2 = (v2 < 0.0f || v2 > 1.0f) ? 0.0f : g_col[2];
         float gd0 = 0.0f, gd1 = 0.0f, gd2 = 0.0f;
-        float4* gsh4 = reinterpret_cast<float4*>(gsh);
 #pragma unroll
         for (int grp = 0; grp < 4; ++grp) {
             float o[12];
             if (4 * grp < n) {
-                const float4 a = __ldg(sh4 + 3 * grp), b = __ldg(sh4 + 3 * grp + 1), c = __ldg(sh4 + 3 * grp + 2);
+                const float4 a = row[(3 * grp) ^ swz], b = row[(3 * grp + 1) ^ swz], c = row[(3 * grp + 2) ^ swz];
                 const float e[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
@@ -506,9 +513,9 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
 #pragma unroll
                 for (int q = 0; q < 12; ++q) o[q] = 0.0f;
             }
-            gsh4[3 * grp] = make_float4(o[0], o[1], o[2], o[3]);
-            gsh4[3 * grp + 1] = make_float4(o[4], o[5], o[6], o[7]);
-            gsh4[3 * grp + 2] = make_float4(o[8], o[9], o[10], o[11]);
+            row[(3 * grp) ^ swz] = make_float4(o[0], o[1], o[2], o[3]);
+            row[(3 * grp + 1) ^ swz] = make_float4(o[4], o[5], o[6], o[7]);
+            row[(3 * grp + 2) ^ swz] = make_float4(o[8], o[9], o[10], o[11]);
         }
         if (dok) {
             const float dot = gd0 * dx_ + gd1 * dy_ + gd2 * dz_;
@@ -562,6 +569,55 @@ project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRender
     }
 }
 
+/* Per block of 128 Gaussians: the SH rows come in with coalesced
+ * asynchronous 16-byte copies (swizzled rows, see sh_swizzle), each thread
+ * forms its Gaussian's gradients (its dL/dsh in place of its row), and the
+ * rows go out with coalesced 16-byte stores. Culled Gaussians get zeros. */
+__global__ void __launch_bounds__(kProjBwdThreads, 6)
+project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt,
+                        const int* __restrict__ radii, const float* __restrict__ grad2d, LumenGpuGradients out) {
+    chain_begin();
+    __shared__ DevCamera cam_s;
+    extern __shared__ float4 sh_rows[];   /* kProjBwdThreads x 12 chunks */
+    const int tid = threadIdx.x;
+    const long long i0 = (long long)blockIdx.x * kProjBwdThreads;
+    const int nblk = (int)(g.count - i0 < kProjBwdThreads ? g.count - i0 : kProjBwdThreads);
+    {
+        const float4* src = reinterpret_cast<const float4*>(g.sh + i0 * 48);
+        for (int c = tid; c < nblk * 12; c += kProjBwdThreads) {
+            const int t = c / 12, q = c - 12 * t;
+            cp_async16(sh_rows + 12 * t + (q ^ sh_swizzle(t)), src + c);
+        }
+        cp_async_commit();
+    }
+    if (tid == 0) setup_camera(camera, cam_s);
+    const long long i = i0 + tid;
+    const bool visible = tid < nblk && radii[i] > 0;
+    cp_async_wait_all();
+    __syncthreads();
+    float4* row = sh_rows + tid * 12;
+    const int swz = sh_swizzle(tid);
+    if (visible) {
+        project_backward_gaussian(g, cam_s, opt, i, grad2d, out, row, swz);
+    } else if (tid < nblk) {
+        float* gm = out.means + i * 3;
+        float* gs = out.scales + i * 3;
+        float* gq = out.quats + i * 4;
+        gm[0] = gm[1] = gm[2] = 0.0f;
+        gs[0] = gs[1] = gs[2] = 0.0f;
+        gq[0] = gq[1] = gq[2] = gq[3] = 0.0f;
+        out.opacities[i] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) row[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    __syncthreads();
+    float4* dst = reinterpret_cast<float4*>(out.sh + i0 * 48);
+    for (int c = tid; c < nblk * 12; c += kProjBwdThreads) {
+        const int t = c / 12, q = c - 12 * t;
+        dst[c] = sh_rows[12 * t + (q ^ sh_swizzle(t))];
+    }
+}
+
 /* ---------------------------------------------------------------- K8 -- */
 
 constexpr int kL1Blocks = 1024;
@@ -610,9 +666,67 @@ __global__ void l1_finish_kernel(const float* __restrict__ partial, long long n,
 using namespace lumen;
 
 namespace lumen {
+
+/* The compositing adjoint's shared memory is above the 48 KB default; set
+ * per device by configure_once. */
+void configure_backward_kernels() {
+    cudaFuncSetAttribute(composite_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmemBytes);
+    /* four 55.6 KB CTAs per SM need the largest shared-memory carveout */
+    cudaFuncSetAttribute(composite_backward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+}
+
+void configure_once();
 LumenStatus check_inputs(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt);
 LumenStatus map_cuda(cudaError_t e);
+cudaEvent_t* stage_timer_take(LumenGpuStageTimer* t);
+
+/* timer: a stage timer whose next frame receives five events (start,
+ * after the compositing adjoint, then three after the projection adjoint),
+ * taken once the arguments are valid; or nullptr. */
+static LumenStatus backward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                 const LumenRenderOptions* opt, const LumenGpuFrame* f,
+                                 const LumenGpuImage* fwd, const float* grad_rgb, const float* grad_depth,
+                                 const float* grad_alpha, LumenGpuGradients* out, LumenGpuStageTimer* timer,
+                                 void* stream) {
+    LumenStatus st = check_inputs(g, cam, opt);
+    if (st != LUMEN_SUCCESS) return st;
+    if (!f || !f->scratch || !grad_rgb || !out || !fwd || !fwd->rgb || !fwd->alpha || !fwd->last_idx)
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (grad_depth && opt->compute_depth && !fwd->depth) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (g->count > 0 &&
+        (!out->means || !out->scales || !out->quats || !out->opacities || !out->sh || !out->splat2d ||
+         !f->records || !f->visible_ids || !f->radii || !f->ranges || !f->vals[0] || !f->vals[1] ||
+         ((uintptr_t)out->splat2d & 15u) != 0))
+        return LUMEN_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    configure_once();
+    cudaEvent_t* ev = nullptr;
+    if (timer && !(ev = stage_timer_take(timer))) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (g->count == 0) {
+        if (ev)
+            for (int k = 0; k < 5; ++k) cudaEventRecord(ev[k], s);
+        return LUMEN_SUCCESS;
+    }
+    Control* ctrl = (Control*)f->scratch;
+    if (ev) cudaEventRecord(ev[0], s);
+    cudaError_t e = cudaMemsetAsync(out->splat2d, 0, (size_t)g->count * kGrad2DStride * sizeof(float), s);
+    if (e != cudaSuccess) return map_cuda(e);
+    const int tiles_x = (cam->width + kTile - 1) / kTile;
+    const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
+    launch_chained(composite_backward_kernel, dim3(tiles), dim3(kTilePixels), kBwdSmemBytes, s,
+                   (const LumenSplatRecord*)f->records, *f, ctrl, cam->width, cam->height, tiles_x, *opt,
+                   (const float*)fwd->rgb, (const float*)fwd->depth, (const float*)fwd->alpha,
+                   (const int*)fwd->last_idx, grad_rgb, grad_depth, grad_alpha, out->splat2d);
+    if (ev) cudaEventRecord(ev[1], s);
+    const long long nb = (g->count + kProjBwdThreads - 1) / kProjBwdThreads;
+    launch_chained(project_backward_kernel, dim3((unsigned int)nb), dim3(kProjBwdThreads), kProjBwdStageBytes, s,
+                   *g, *cam, *opt, (const int*)f->radii, (const float*)out->splat2d, *out);
+    if (ev)
+        for (int k = 2; k < 5; ++k) cudaEventRecord(ev[k], s);
+    return map_cuda(cudaGetLastError());
 }
+}  // namespace lumen
 
 extern "C" {
 
@@ -620,30 +734,16 @@ LumenStatus lumen_gpu_render_backward(const LumenGpuGaussians* g, const LumenVie
                                       const LumenRenderOptions* opt, const LumenGpuFrame* f,
                                       const LumenGpuImage* fwd, const float* grad_rgb, const float* grad_depth,
                                       const float* grad_alpha, LumenGpuGradients* out, void* stream) {
-    LumenStatus st = check_inputs(g, cam, opt);
-    if (st != LUMEN_SUCCESS) return st;
-    if (!f || !f->scratch || !grad_rgb || !out || !fwd || !fwd->rgb || !fwd->alpha || !fwd->last_idx)
-        return LUMEN_ERROR_INVALID_ARGUMENT;
-    if (grad_depth && opt->compute_depth && !fwd->depth) return LUMEN_ERROR_INVALID_ARGUMENT;
-    if (g->count == 0) return LUMEN_SUCCESS;
-    if (!out->means || !out->scales || !out->quats || !out->opacities || !out->sh || !out->splat2d ||
-        !f->records || !f->visible_ids || !f->radii || !f->ranges || !f->vals[0] || !f->vals[1])
-        return LUMEN_ERROR_INVALID_ARGUMENT;
-    cudaStream_t s = (cudaStream_t)stream;
-    Control* ctrl = (Control*)f->scratch;
-    if (((uintptr_t)out->splat2d & 15u) != 0) return LUMEN_ERROR_INVALID_ARGUMENT;
-    cudaError_t e = cudaMemsetAsync(out->splat2d, 0, (size_t)g->count * kGrad2DStride * sizeof(float), s);
-    if (e != cudaSuccess) return map_cuda(e);
-    const int tiles_x = (cam->width + kTile - 1) / kTile;
-    const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
-    launch_chained(composite_backward_kernel, dim3(tiles), dim3(kTilePixels), 0, s,
-                   (const LumenSplatRecord*)f->records, *f, ctrl, cam->width, cam->height, tiles_x, *opt,
-                   (const float*)fwd->rgb, (const float*)fwd->depth, (const float*)fwd->alpha,
-                   (const int*)fwd->last_idx, grad_rgb, grad_depth, grad_alpha, out->splat2d);
-    const long long nb = (g->count + 255) / 256;
-    launch_chained(project_backward_kernel, dim3((unsigned int)nb), dim3(256), 0, s, *g, *cam, *opt,
-                   (const int*)f->radii, (const float*)out->splat2d, *out);
-    return map_cuda(cudaGetLastError());
+    return backward_impl(g, cam, opt, f, fwd, grad_rgb, grad_depth, grad_alpha, out, nullptr, stream);
+}
+
+LumenStatus lumen_gpu_render_backward_timed(const LumenGpuGaussians* g, const LumenViewCamera* cam,
+                                            const LumenRenderOptions* opt, const LumenGpuFrame* f,
+                                            const LumenGpuImage* fwd, const float* grad_rgb, const float* grad_depth,
+                                            const float* grad_alpha, LumenGpuGradients* out,
+                                            LumenGpuStageTimer* timer, void* stream) {
+    if (!timer) return LUMEN_ERROR_INVALID_ARGUMENT;
+    return backward_impl(g, cam, opt, f, fwd, grad_rgb, grad_depth, grad_alpha, out, timer, stream);
 }
 
 size_t lumen_gpu_l1_loss_scratch_bytes(void) { return (size_t)kL1Blocks * sizeof(float); }

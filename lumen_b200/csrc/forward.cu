@@ -58,6 +58,7 @@ int device_sm_count() {
 }
 
 void prime_persistent_launches();
+void configure_backward_kernels();
 
 /* Kernel attributes (the large dynamic shared memory limits) apply to the
  * device that is current when they are set, so they are set once per
@@ -71,11 +72,13 @@ void configure_once() {
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxConfiguredDevices) {
         configure_sort_kernels();
         prime_persistent_launches();
+        configure_backward_kernels();
         return;
     }
     std::call_once(once[dev], [] {
         configure_sort_kernels();
         prime_persistent_launches();
+        configure_backward_kernels();
     });
 }
 
@@ -165,9 +168,10 @@ __global__ void frame_init_kernel(unsigned long long* zero, long long n_words, V
  * n_tiles are the batch's (plain launches) or upper bounds (persistent
  * launches, whose kernels read the batch's sizes from the table); n_views
  * is the batch's view count, or 0 when only the table knows it; n_units
- * the batch's projection units (plain launches of several views). A single
- * view is projected with its compacting scan fused in (project_kernel);
- * several views Gaussian-major, each distinct scene read once. */
+ * the projection units (plain launches). Projection is a visibility count,
+ * an offset scan and the projection proper, Gaussian-major (each distinct
+ * scene read once); with n_units 0 a single view instead runs the one-pass
+ * kernel with its compacting scan fused in (project_kernel). */
 void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRenderOptions& opt,
                      const LumenGpuFrame& f, long long n_slots, long long n_tiles, int n_views, bool persistent,
                      const LaunchConfig& lc, cudaEvent_t* ev, cudaStream_t s, bool with_composite,
@@ -180,7 +184,7 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
     unsigned int* tile_lb = (unsigned int*)(base + L.tile_lb_off);
     const int sms = device_sm_count();
     if (n_slots > 0) {
-        if (n_views == 1)
+        if (n_views == 1 && n_units == 0)
             launch_project(vt, n_views, opt, f, ctrl, proj_lb, L.proj_blocks, persistent, sms, s);
         else
             launch_batch_project(vt, opt, f, ctrl, proj_lb, n_units, persistent, sms, s);
@@ -228,6 +232,26 @@ static bool launch_ok(const LaunchConfig& lc) {
            (lc.tile_sort_items == 8 || lc.tile_sort_items == 16 || lc.tile_sort_items == 24);
 }
 
+/* The one-view table of a plain frame: the view leads its own scene group
+ * and owns every projection unit. */
+static void single_view_table(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenGpuImage* img,
+                              const ScratchLayout& L, long long tiles, BatchHeader* hdr, ViewDesc* v) {
+    std::memset(hdr, 0, sizeof(*hdr));
+    hdr->n_views = 1;
+    hdr->total_blocks = L.proj_blocks;
+    hdr->total_tiles = tiles;
+    hdr->total_units = L.proj_blocks;
+    std::memset(v, 0, sizeof(*v));
+    v->g = *g;
+    v->cam = *cam;
+    v->tiles_x = (cam->width + kTile - 1) / kTile;
+    v->img = *img;
+    v->inst_begin = -1;
+    v->unit_begin = 0;
+    v->group_next = -1;
+    v->group_lead = 1;
+}
+
 static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
                                 LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream,
                                 const LaunchConfig& lc = kDefaultLaunch) {
@@ -243,20 +267,11 @@ static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamer
     const int tiles_x = (cam->width + kTile - 1) / kTile;
     const long long tiles = (long long)tiles_x * ((cam->height + kTile - 1) / kTile);
     BatchHeader hdr{};
-    hdr.n_views = 1;
-    hdr.total_blocks = L.proj_blocks;
-    hdr.total_tiles = tiles;
     ViewDesc v{};
-    v.g = *g;
-    v.cam = *cam;
-    v.tiles_x = tiles_x;
-    v.img = *img;
-    v.block_begin = 0;
-    v.tile_begin = 0;
-    v.inst_begin = -1;
+    single_view_table(g, cam, img, L, tiles, &hdr, &v);
     if (ev) cudaEventRecord(ev[0], s);
     launch_init(L, base, &hdr, &v, s);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s, true, 0);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, ev, s, true, hdr.total_units);
     return map_cuda(cudaGetLastError());
 }
 
@@ -279,17 +294,11 @@ LumenStatus forward_banded(const LumenGpuGaussians* g, const LumenViewCamera* ca
     const int tiles_y = (cam->height + kTile - 1) / kTile;
     const long long tiles = (long long)tiles_x * tiles_y;
     BatchHeader hdr{};
-    hdr.n_views = 1;
-    hdr.total_blocks = L.proj_blocks;
-    hdr.total_tiles = tiles;
     ViewDesc v{};
-    v.g = *g;
-    v.cam = *cam;
-    v.tiles_x = tiles_x;
-    v.img = *img;
-    v.inst_begin = -1;
+    single_view_table(g, cam, img, L, tiles, &hdr, &v);
     launch_init(L, base, &hdr, &v, s);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, nullptr, s, false, 0);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, nullptr, s, false,
+                    hdr.total_units);
     Control* ctrl = (Control*)(base + L.control_off);
     const ViewTable* vt = (const ViewTable*)(base + L.table_off);
     const int sms = device_sm_count();
@@ -492,6 +501,19 @@ LumenStatus lumen_gpu_render_batch_timed(const LumenGpuBatchView* views, int32_t
     if (st == LUMEN_SUCCESS) t->next++;
     return st;
 }
+
+}  // extern "C"
+
+namespace lumen {
+/* The next frame's five events of a stage timer, or nullptr when it is full
+ * (used by the timed backward). The caller records all five. */
+cudaEvent_t* stage_timer_take(LumenGpuStageTimer* t) {
+    if (!t || t->next >= t->max_frames) return nullptr;
+    return t->ev + (size_t)(t->next++) * 5;
+}
+}  // namespace lumen
+
+extern "C" {
 
 LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* t, float stage_ms[4], float* total_ms, int* n_frames) {
     if (!t || !stage_ms) return LUMEN_ERROR_INVALID_ARGUMENT;

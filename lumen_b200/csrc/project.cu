@@ -92,7 +92,10 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
         {
             const int nblk = (int)(count - i0 < kProjThreads ? count - i0 : kProjThreads);
             const float4* src = reinterpret_cast<const float4*>(s.vd.g.sh + i0 * 48);
-            for (int c = tid; c < nblk * 12; c += kProjThreads) cp_async16(sh_stage + c, src + c);
+            for (int c = tid; c < nblk * 12; c += kProjThreads) {
+                const int t = c / 12, q = c - 12 * t;
+                cp_async16(sh_stage + 12 * t + (q ^ sh_swizzle(t)), src + c);
+            }
             cp_async_commit();
         }
         float mx = 0.0f, my = 0.0f, mz = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f, op = 0.0f;
@@ -114,7 +117,7 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
         p.radius = 0;
         if (i < count) {
             p = project_gaussian(s.vd.dcam, mx, my, mz, sx, sy, sz, Quat{q.x, q.y, q.z, q.w}, op,
-                                 reinterpret_cast<const float*>(sh_stage + tid * 12), opt);
+                                 reinterpret_cast<const float*>(sh_stage + tid * 12), opt, sh_swizzle(tid));
             if (f.radii) f.radii[slot] = p.visible ? p.radius : 0;
         }
         unsigned int block_vis = 0;
@@ -513,7 +516,10 @@ batch_project_kernel(const ViewTable* __restrict__ vt, LumenRenderOptions opt, L
             const long long count = g.count;
             const int nblk = (int)(count - i0 < kProjThreads ? count - i0 : kProjThreads);
             const float4* src = reinterpret_cast<const float4*>(g.sh + i0 * 48);
-            for (int c = tid; c < nblk * 12; c += kProjThreads) cp_async16(sh_stage + c, src + c);
+            for (int c = tid; c < nblk * 12; c += kProjThreads) {
+                const int t = c / 12, q = c - 12 * t;
+                cp_async16(sh_stage + 12 * t + (q ^ sh_swizzle(t)), src + c);
+            }
             cp_async_commit();
         }
         const UnitParams up = load_unit_params(g, i, opt);
@@ -524,7 +530,8 @@ batch_project_kernel(const ViewTable* __restrict__ vt, LumenRenderOptions opt, L
             copy_camera(s.cam, vt->view[v].dcam);
             __syncthreads();
             const Projected p = project_prepared<true>(s.cam, up.mx, up.my, up.mz, up.pr,
-                                                       reinterpret_cast<const float*>(sh_stage + tid * 12), opt);
+                                                       reinterpret_cast<const float*>(sh_stage + tid * 12), opt,
+                                                       sh_swizzle(tid));
             const long long blk = vt->view[v].block_begin + b;
             if (f.radii && in_scene) f.radii[blk * kProjThreads + tid] = p.visible ? p.radius : 0;
             unsigned int n_vis = 0;

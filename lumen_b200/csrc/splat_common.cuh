@@ -324,11 +324,18 @@ struct Projected {
     bool visible;
 };
 
+/* A Gaussian's SH row staged in shared memory as 12 16-byte chunks: chunk
+ * q of row t sits at 12 t + (q ^ sh_swizzle(t)). Rows are 48 words apart,
+ * so without the swizzle the 8 lanes of each phase of a 16-byte load hit
+ * only 2 of the 8 chunk slots of the 32 banks (a 4-way conflict); the XOR
+ * spreads them over all 8, and it keeps every chunk in its row. */
+__device__ __forceinline__ int sh_swizzle(int t) { return (t >> 1) & 3; }
+
 /* SHBasis.evaluate + evaluate_sh_color, spherical_harmonics.mojo:68-111,133-172;
  * sh points at the Gaussian's 48 coefficients (16-byte aligned; the
- * projection kernel stages them in shared memory). */
+ * projection kernels stage them in shared memory, chunk q at q ^ swz). */
 __device__ __forceinline__ void sh_color(const float* __restrict__ sh, float dx0, float dy0, float dz0,
-                                         int degree, float& r, float& g, float& b) {
+                                         int degree, float& r, float& g, float& b, int swz = 0) {
     const float C0 = (float)0.28209479177387814, C1 = (float)0.4886025119029199;
     const float C2_0 = (float)1.0925484305920792, C2_1 = (float)0.31539156525252005;
     const float C2_2 = (float)0.5462742152960396, C3_0 = (float)0.5900435899266435;
@@ -364,7 +371,7 @@ __device__ __forceinline__ void sh_color(const float* __restrict__ sh, float dx0
     float c[48];
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-        float4 v = s4[k];
+        float4 v = s4[k ^ swz];
         c[4 * k + 0] = v.x; c[4 * k + 1] = v.y; c[4 * k + 2] = v.z; c[4 * k + 3] = v.w;
     }
     float rr = 0.5f, gg = 0.5f, bb = 0.5f;
@@ -426,7 +433,7 @@ __device__ __forceinline__ Prepared prepare_gaussian(float sx, float sy, float s
 template <bool kFull = true>
 __device__ __forceinline__ Projected project_prepared(const DevCamera& cam, float mx, float my, float mz,
                                                       const Prepared& pr, const float* __restrict__ sh,
-                                                      const LumenRenderOptions& o) {
+                                                      const LumenRenderOptions& o, int sh_swz = 0) {
     Projected p;
     p.visible = false;
     p.radius = 0;
@@ -497,7 +504,7 @@ __device__ __forceinline__ Projected project_prepared(const DevCamera& cam, floa
     float vl = sqrtf(vx * vx + vy * vy + vz * vz);
     float dx = 0.0f, dy = 0.0f, dz = 0.0f;
     if (vl > (float)0.000001) { dx = vx / vl; dy = vy / vl; dz = vz / vl; }
-    sh_color(sh, dx, dy, dz, o.sh_degree, p.r, p.g, p.b);
+    sh_color(sh, dx, dy, dz, o.sh_degree, p.r, p.g, p.b, sh_swz);
     /* Covariance2D.inverse, projection.mojo:30-42 */
     float det = c00 * c11 - c01 * c01;
     if (det > (float)-0.0000001 && det < (float)0.0000001) {
@@ -516,8 +523,9 @@ __device__ __forceinline__ Projected project_prepared(const DevCamera& cam, floa
  * Follows pipeline.mojo:85-149 and the functions it calls. */
 __device__ __forceinline__ Projected project_gaussian(const DevCamera& cam, float mx, float my, float mz,
                                                       float sx, float sy, float sz, Quat qraw, float op,
-                                                      const float* __restrict__ sh, const LumenRenderOptions& o) {
-    return project_prepared<true>(cam, mx, my, mz, prepare_gaussian(sx, sy, sz, qraw, op, o), sh, o);
+                                                      const float* __restrict__ sh, const LumenRenderOptions& o,
+                                                      int sh_swz = 0) {
+    return project_prepared<true>(cam, mx, my, mz, prepare_gaussian(sx, sy, sz, qraw, op, o), sh, o, sh_swz);
 }
 
 /* float_to_ordered_uint32 (radix_sort.mojo:8-18) or the raw float bits. */
