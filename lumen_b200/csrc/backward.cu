@@ -46,26 +46,24 @@ namespace lumen {
 
 constexpr int kGrad2D = 10;   /* cx, cy, ic00, ic01, ic11, opacity, r, g, b, depth */
 constexpr int kGrad2DStride = 12;   /* floats per Gaussian in splat2d: 16-byte rows for vector atomics */
-constexpr int kBwdChunk = kTilePixels;   /* instances staged per round (list entries fit a byte) */
-static_assert(kBwdChunk <= 256, "warp lists hold byte offsets");
-/* Warp sums are formed for three splats at a time: lane l writes its 10
- * values of splat u to row l, columns 10 u .. 10 u + 9 of a 32 x 30 buffer;
- * lane c < 30 then adds column c (value c % 10 of splat c / 10). */
-constexpr int kRedSplats = 3;
-constexpr int kRedCols = kRedSplats * kGrad2D;
-constexpr int kRedWords = 32 * kRedCols;
+constexpr int kBwdChunk = kTilePixels;   /* instances staged per round */
+/* per warp: 32 rows of kGrad2D values (5 pairs), then zero padding up to
+ * the last word a lane of the transposed read touches (2 * 31 + 60 * 5 + 1) */
+constexpr int kRedRows = 32 * kGrad2D;
+constexpr int kRedWords = 364;
+constexpr int kRedReads = 6;
 
 struct BackwardSmem {
     float4 geo[kBwdChunk];        /* cx, cy, depth, opacity */
     float4 con[kBwdChunk];        /* 0.5 ic00, ic01, 0.5 ic11, - (the forward's prescaled conic) */
     float4 col[kBwdChunk];        /* r, g, b, - */
     unsigned char mask[kBwdChunk];
-    unsigned char list[kTilePixels / 32][kBwdChunk];
+    unsigned short list[kTilePixels / 32][kBwdChunk];
     float acc[kBwdChunk][kGrad2D];
+    unsigned int gid[kBwdChunk];
     float red[kTilePixels / 32][kRedWords];
     int tile_last;
 };
-constexpr size_t kBwdSmemBytes = sizeof(BackwardSmem);
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
@@ -93,6 +91,7 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
             s.geo[tid] = geo;
             s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
             s.col[tid] = __ldg(r4 + 2);
+            s.gid[tid] = visible_ids[v];
             m = reach_mask(geo, con, tile_x0, tile_y0);
         }
     }
@@ -106,33 +105,11 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
         const int j = base + lane;
         const bool bit = j < n && ((s.mask[j] >> warp) & 1u);
         const unsigned int bal = __ballot_sync(0xffffffffu, bit);
-        if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned char)j;
+        if (bit) s.list[warp][cnt + __popc(bal & lanemask_lt())] = (unsigned short)j;
         cnt += __popc(bal);
     }
     __syncwarp();
     return cnt;
-}
-
-/* The buffered splats' warp sums (n of them, columns 10 u .. 10 u + 9 of
- * splat u), added to the CTA's accumulators. */
-__device__ __forceinline__ void flush_warp_sums(BackwardSmem& s, const float* red, int n, int j0, int j1, int j2) {
-    const int lane = threadIdx.x & 31;
-    __syncwarp();
-    if (lane < kGrad2D * n) {
-        float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
-#pragma unroll
-        for (int r = 0; r < 32; r += 4) {
-            a0 += red[kRedCols * r + lane];
-            a1 += red[kRedCols * (r + 1) + lane];
-            a2 += red[kRedCols * (r + 2) + lane];
-            a3 += red[kRedCols * (r + 3) + lane];
-        }
-        const float sum = (a0 + a1) + (a2 + a3);
-        const int u = lane >= 2 * kGrad2D ? 2 : lane >= kGrad2D ? 1 : 0;
-        const int j = u == 0 ? j0 : u == 1 ? j1 : j2;
-        if (sum != 0.0f) atomicAdd(&s.acc[j][lane - kGrad2D * u], sum);
-    }
-    __syncwarp();
 }
 
 /* The hardware exponential of -p (p in [0, 4.5]): within a few parts per
@@ -149,7 +126,7 @@ __device__ __forceinline__ float fast_rcp(float x) {
     return r;
 }
 
-__global__ void __launch_bounds__(kTilePixels, 4)
+__global__ void __launch_bounds__(kTilePixels, 5)
 composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpuFrame f, Control* ctrl,
                           int width, int height, int tiles_x, LumenRenderOptions opt,
                           const float* __restrict__ out_rgb, const float* __restrict__ out_depth,
@@ -157,8 +134,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                           const float* __restrict__ grad_rgb, const float* __restrict__ grad_depth,
                           const float* __restrict__ grad_alpha, float* __restrict__ grad2d) {
     chain_begin();
-    extern __shared__ __align__(16) unsigned char bwd_smem[];
-    BackwardSmem& s = *reinterpret_cast<BackwardSmem*>(bwd_smem);
+    __shared__ BackwardSmem s;
     const int tile = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
@@ -184,6 +160,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     float g_r = 0.0f, g_g = 0.0f, g_b = 0.0f, g_d = 0.0f, Gc = 0.0f;
     int last = -1;
     if (tid == 0) s.tile_last = -1;
+    for (int w = kRedRows + lane; w < kRedWords; w += 32) s.red[warp][w] = 0.0f;
     if (inside) {
         last = out_last[pix];
         if (last >= re) {   /* self-check: a last-visited instance beyond the tile's range */
@@ -207,6 +184,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
         Gc = g_r * (out_rgb[pix * 3 + 0] - bg) + g_g * (out_rgb[pix * 3 + 1] - bg) +
              g_b * (out_rgb[pix * 3 + 2] - bg) + g_d * C_z - g_tail;
     }
+    const float2 G_rg = make_float2(g_r, g_g), G_bz = make_float2(g_b, g_d);
     /* the tile's sweep ends at the last instance any of its pixels visited */
     const int wlast = __reduce_max_sync(0xffffffffu, last);
     __syncthreads();
@@ -219,12 +197,12 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
     float* red = s.red[warp];
     for (int cs = rs; cs < end; cs += kBwdChunk) {
         const int cnt = stage_chunk(s, records, vals, f.visible_ids, n_visible, ctrl, cs, end, tile_x0, tile_y0);
-        int nbuf = 0, j0 = 0, j1 = 0, j2 = 0;   /* splats buffered for the warp sums (warp-uniform) */
         for (int t = 0; t < cnt; ++t) {
             const int j = s.list[warp][t];
             if (cs + j > wlast) break;   /* every pixel of the warp is past its last splat */
-            float gcx = 0.0f, gcy = 0.0f, ga = 0.0f, gb = 0.0f, gc = 0.0f, gop = 0.0f;
-            float gr = 0.0f, gg_ = 0.0f, gbl = 0.0f, gz = 0.0f;
+            float2 g_xy = make_float2(0.0f, 0.0f), g_ac = make_float2(0.0f, 0.0f);
+            float2 g_rg = make_float2(0.0f, 0.0f), g_bz = make_float2(0.0f, 0.0f);
+            float gb = 0.0f, gop = 0.0f;
             bool contrib = false;
             if (cs + j <= last) {
                 const float4 geo = s.geo[j], cc = s.con[j];
@@ -249,11 +227,13 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                         contrib = true;
                         const float4 col = s.col[j];
                         const float w = alpha * T;
-                        gr = g_r * w;
-                        gg_ = g_g * w;
-                        gbl = g_b * w;
-                        gz = g_d * w;
-                        const float gcol = g_r * col.x + g_g * col.y + g_b * col.z + g_d * geo.z;
+                        /* two-wide packed arithmetic: (r, g), (b, depth), (x, y) */
+                        const float2 ww = make_float2(w, w);
+                        g_rg = __fmul2_rn(G_rg, ww);
+                        g_bz = __fmul2_rn(G_bz, ww);
+                        const float2 gc2 = __ffma2_rn(G_bz, make_float2(col.z, geo.z),
+                                                      __fmul2_rn(G_rg, make_float2(col.x, col.y)));
+                        const float gcol = gc2.x + gc2.y;
                         GP += w * gcol;
                         const float one_minus = 1.0f - alpha;
                         const float dalpha = T * gcol - (Gc - GP) * fast_rcp(one_minus);
@@ -262,39 +242,59 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                             gop = dalpha * gexp;
                             if (!pclamp) {
                                 const float dpower = -gop * geo.w;
-                                const float dxp = dx * dpower;
-                                ga = 0.5f * dx * dxp;
-                                gb = dy * dxp;
-                                gc = 0.5f * dy * dy * dpower;
+                                const float2 d = make_float2(dx, dy);
+                                /* (0.5 dx^2, 0.5 dy^2) dpower and dx dy dpower */
+                                g_ac = __fmul2_rn(__fmul2_rn(d, d), make_float2(0.5f * dpower, 0.5f * dpower));
+                                gb = dx * dy * dpower;
                                 /* d dx / d cx = -1; the staged conic holds 0.5 a and 0.5 c */
-                                gcx = -(2.0f * cc.x * dx + cc.y * dy) * dpower;
-                                gcy = -(cc.y * dx + 2.0f * cc.z * dy) * dpower;
+                                const float2 u = __ffma2_rn(make_float2(cc.y, 2.0f * cc.z), make_float2(dy, dy),
+                                                            __fmul2_rn(make_float2(2.0f * cc.x, cc.y), make_float2(dx, dx)));
+                                g_xy = __fmul2_rn(u, make_float2(-dpower, -dpower));
                             }
                         }
                     }
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
-                float2* row = reinterpret_cast<float2*>(red + lane * kRedCols + kGrad2D * nbuf);
-                row[0] = make_float2(gcx, gcy);
-                row[1] = make_float2(ga, gb);
-                row[2] = make_float2(gc, gop);
-                row[3] = make_float2(gr, gg_);
-                row[4] = make_float2(gbl, gz);
-                if (nbuf == 0) j0 = j; else if (nbuf == 1) j1 = j; else j2 = j;
-                if (++nbuf == kRedSplats) {
-                    flush_warp_sums(s, red, nbuf, j0, j1, j2);
-                    nbuf = 0;
+                /* warp sum by a shared-memory transpose: row `lane` holds this
+                 * lane's 10 values as 5 pairs; lane l < 30 adds pair l % 5 of
+                 * rows l / 5, l / 5 + 6, ... (packed adds), then two shuffle
+                 * steps combine the six partial sums of each pair */
+                float2* row = reinterpret_cast<float2*>(red + lane * kGrad2D);
+                row[0] = g_xy;
+                row[1] = make_float2(g_ac.x, gb);
+                row[2] = make_float2(g_ac.y, gop);
+                row[3] = g_rg;
+                row[4] = g_bz;
+                __syncwarp();
+                const float2* rd = reinterpret_cast<const float2*>(red) + lane;
+                float2 sum = rd[0];
+#pragma unroll
+                for (int r = 1; r < kRedReads; ++r) sum = __fadd2_rn(sum, rd[30 * r]);
+                /* part q (lanes 5 q .. 5 q + 4): first q + (q + 3) for q < 3,
+                 * then lane p < 5 adds parts 1 and 2 of those sums */
+                float2 o, o2;
+                o.x = __shfl_down_sync(0xffffffffu, sum.x, 15);
+                o.y = __shfl_down_sync(0xffffffffu, sum.y, 15);
+                sum = __fadd2_rn(sum, o);
+                o.x = __shfl_down_sync(0xffffffffu, sum.x, 5);
+                o.y = __shfl_down_sync(0xffffffffu, sum.y, 5);
+                o2.x = __shfl_down_sync(0xffffffffu, sum.x, 10);
+                o2.y = __shfl_down_sync(0xffffffffu, sum.y, 10);
+                sum = __fadd2_rn(sum, __fadd2_rn(o, o2));
+                /* lane p < 5 holds values 2 p and 2 p + 1 */
+                if (lane < kGrad2D / 2) {
+                    if (sum.x != 0.0f) atomicAdd(&s.acc[j][2 * lane], sum.x);
+                    if (sum.y != 0.0f) atomicAdd(&s.acc[j][2 * lane + 1], sum.y);
                 }
+                __syncwarp();
             }
         }
-        if (nbuf) flush_warp_sums(s, red, nbuf, j0, j1, j2);
         __syncthreads();
         /* per (splat, tile): three vector atomics (4 + 4 + 2 values) */
         const int i = cs + tid;
-        const unsigned int v = i < end ? vals[i] : n_visible;
-        if (v < n_visible) {
-            float* dst = grad2d + (size_t)f.visible_ids[v] * kGrad2DStride;
+        if (i < end) {
+            float* dst = grad2d + (size_t)s.gid[tid] * kGrad2DStride;
             const float* a = s.acc[tid];
             if (a[0] != 0.0f || a[1] != 0.0f || a[2] != 0.0f || a[3] != 0.0f)
                 atomicAdd(reinterpret_cast<float4*>(dst), make_float4(a[0], a[1], a[2], a[3]));
@@ -667,11 +667,9 @@ using namespace lumen;
 
 namespace lumen {
 
-/* The compositing adjoint's shared memory is above the 48 KB default; set
- * per device by configure_once. */
+/* Five 39.6 KB CTAs of the compositing adjoint per SM need the largest
+ * shared-memory carveout; set per device by configure_once. */
 void configure_backward_kernels() {
-    cudaFuncSetAttribute(composite_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmemBytes);
-    /* four 55.6 KB CTAs per SM need the largest shared-memory carveout */
     cudaFuncSetAttribute(composite_backward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
 }
@@ -714,7 +712,7 @@ static LumenStatus backward_impl(const LumenGpuGaussians* g, const LumenViewCame
     if (e != cudaSuccess) return map_cuda(e);
     const int tiles_x = (cam->width + kTile - 1) / kTile;
     const int tiles = tiles_x * ((cam->height + kTile - 1) / kTile);
-    launch_chained(composite_backward_kernel, dim3(tiles), dim3(kTilePixels), kBwdSmemBytes, s,
+    launch_chained(composite_backward_kernel, dim3(tiles), dim3(kTilePixels), 0, s,
                    (const LumenSplatRecord*)f->records, *f, ctrl, cam->width, cam->height, tiles_x, *opt,
                    (const float*)fwd->rgb, (const float*)fwd->depth, (const float*)fwd->alpha,
                    (const int*)fwd->last_idx, grad_rgb, grad_depth, grad_alpha, out->splat2d);

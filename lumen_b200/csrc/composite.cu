@@ -77,9 +77,11 @@ struct PixelState {
  * 0.99 alpha clamp can apply (without one, alpha = opacity * exp(-power)
  * with exp(-power) <= 1 never exceeds it and the test is left out).
  * kModeAlpha: stop when 1 - T reaches the threshold, else when T falls to
- * it. Either way the arithmetic is the reference's, operation by
+ * it. kTrack: count the blended splats and note where the pixel stopped
+ * (only when the view's image asks for contributor counts or last-visited
+ * offsets). Either way the arithmetic is the reference's, operation by
  * operation. */
-template <int kChunk, bool kClamp, bool kModeAlpha>
+template <int kChunk, bool kClamp, bool kModeAlpha, bool kTrack>
 __device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int warp, int cnt, int cs, float pxc,
                                            float pyc, float thr, PixelState& p) {
     for (int t0 = 0; t0 < cnt; t0 += kVoteGroup) {
@@ -108,16 +110,16 @@ __device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int w
                     p.cb += col.z * w;
                     p.dep += gg.z * w;
                     p.T *= (1.0f - alpha);
-                    ++p.count;
+                    if (kTrack) ++p.count;
                     if (kModeAlpha) {
                         p.acc = 1.0f - p.T;
                         if (p.acc >= thr) {
                             p.done = true;
-                            p.last = cs + j;
+                            if (kTrack) p.last = cs + j;
                         }
                     } else if (p.T <= thr) {
                         p.done = true;
-                        p.last = cs + j;
+                        if (kTrack) p.last = cs + j;
                     }
                 }
             }
@@ -138,9 +140,10 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int view = n_views == 1 ? 0 : find_view_by_tile(vt, n_views, gtile);
     int tx, ty, px, py;
-    bool inside, any_instance;
+    bool inside, any_instance, track;
     {
         const ViewDesc& vd = vt->view[view];
+        track = vd.img.n_contrib != nullptr || vd.img.last_idx != nullptr;
         const int tiles_x = vd.tiles_x;
         const int tile = (int)(gtile - vd.tile_begin);
         tx = tile % tiles_x;
@@ -221,12 +224,22 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
                 cnt = (cnt + kVoteGroup - 1) & ~(kVoteGroup - 1);
                 __syncwarp();
                 PixelState px_state{T, cr, cg, cb, dep, acc, count, last, done};
-                if (clamp) {
-                    if (mode_alpha) blend_list<kChunk, true, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                    else blend_list<kChunk, true, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                if (track) {
+                    if (clamp) {
+                        if (mode_alpha) blend_list<kChunk, true, true, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                        else blend_list<kChunk, true, false, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    } else {
+                        if (mode_alpha) blend_list<kChunk, false, true, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                        else blend_list<kChunk, false, false, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    }
                 } else {
-                    if (mode_alpha) blend_list<kChunk, false, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                    else blend_list<kChunk, false, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    if (clamp) {
+                        if (mode_alpha) blend_list<kChunk, true, true, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                        else blend_list<kChunk, true, false, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    } else {
+                        if (mode_alpha) blend_list<kChunk, false, true, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                        else blend_list<kChunk, false, false, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    }
                 }
                 T = px_state.T; cr = px_state.cr; cg = px_state.cg; cb = px_state.cb; dep = px_state.dep;
                 acc = px_state.acc; count = px_state.count; last = px_state.last; done = px_state.done;

@@ -27,8 +27,8 @@
 
 namespace lumen {
 void launch_batch_project(const ViewTable* vt, const LumenRenderOptions& opt, const LumenGpuFrame& f,
-                          Control* ctrl, unsigned long long* lb, long long n_units, bool persistent, int num_sms,
-                          cudaStream_t st);
+                          Control* ctrl, unsigned long long* lb, long long n_units, long long n_blocks,
+                          bool persistent, int num_sms, cudaStream_t st);
 void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& opt, const LumenGpuFrame& f,
                     Control* ctrl, unsigned long long* lb, long long n_blocks, bool persistent, int num_sms,
                     cudaStream_t st);
@@ -187,7 +187,7 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
         if (n_views == 1 && n_units == 0)
             launch_project(vt, n_views, opt, f, ctrl, proj_lb, L.proj_blocks, persistent, sms, s);
         else
-            launch_batch_project(vt, opt, f, ctrl, proj_lb, n_units, persistent, sms, s);
+            launch_batch_project(vt, opt, f, ctrl, proj_lb, n_units, L.proj_blocks, persistent, sms, s);
         if (ev) cudaEventRecord(ev[1], s);
         launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
                       &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,

@@ -357,8 +357,10 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
 constexpr int kCamWords = (int)(sizeof(DevCamera) / 4);
 static_assert(sizeof(DevCamera) % 4 == 0 && kCamWords <= kProjThreads, "camera copy layout");
 constexpr int kOffsetsThreads = 256;
-constexpr int kOffsetsItems = 8;
+constexpr int kOffsetsItems = 32;   /* 8192 counts per tile: one tile for a 1M-Gaussian view */
 constexpr int kOffsetsTile = kOffsetsThreads * kOffsetsItems;
+/* resident projection CTAs per SM: 64 registers, 8 x 24.6 KB of staged SH rows */
+constexpr int kBatchProjectCtas = 8;
 
 struct BatchProjSmem {
     DevCamera cam;
@@ -489,7 +491,7 @@ batch_offsets_kernel(const ViewTable* __restrict__ vt, Control* ctrl, unsigned l
 }
 
 template <bool kPersistent>
-__global__ void __launch_bounds__(kProjThreads)
+__global__ void __launch_bounds__(kProjThreads, kBatchProjectCtas)
 batch_project_kernel(const ViewTable* __restrict__ vt, LumenRenderOptions opt, LumenGpuFrame f, Control* ctrl,
                      const unsigned long long* lb) {
     chain_begin();
@@ -600,25 +602,25 @@ void prime_persistent_launches() {
  * (plain launches: one CTA per unit) or 0 for persistent launches, which
  * read the count from the table. */
 void launch_batch_project(const ViewTable* vt, const LumenRenderOptions& opt, const LumenGpuFrame& f,
-                          Control* ctrl, unsigned long long* lb, long long n_units, bool persistent, int num_sms,
-                          cudaStream_t st) {
+                          Control* ctrl, unsigned long long* lb, long long n_units, long long n_blocks,
+                          bool persistent, int num_sms, cudaStream_t st) {
     if (persistent) {
         const int pc = g_batch_count_per_sm > 0 ? g_batch_count_per_sm : 1;
         launch_chained(batch_count_kernel<true>, dim3(pc * num_sms), dim3(kProjThreads), 0, st, vt, opt, ctrl, lb);
-    } else {
-        if (n_units <= 0) return;
-        launch_chained(batch_count_kernel<false>, dim3((unsigned int)n_units), dim3(kProjThreads), 0, st, vt, opt,
-                       ctrl, lb);
-    }
-    launch_chained(batch_offsets_kernel, dim3(2 * num_sms), dim3(kOffsetsThreads), 0, st, vt, ctrl, lb);
-    if (persistent) {
+        launch_chained(batch_offsets_kernel, dim3(2 * num_sms), dim3(kOffsetsThreads), 0, st, vt, ctrl, lb);
         const int pp = g_batch_project_per_sm > 0 ? g_batch_project_per_sm : 1;
         launch_chained(batch_project_kernel<true>, dim3(pp * num_sms), dim3(kProjThreads), kProjStageBytes, st, vt,
                        opt, f, ctrl, (const unsigned long long*)lb);
-    } else {
-        launch_chained(batch_project_kernel<false>, dim3((unsigned int)n_units), dim3(kProjThreads), kProjStageBytes,
-                       st, vt, opt, f, ctrl, (const unsigned long long*)lb);
+        return;
     }
+    if (n_units <= 0) return;
+    const long long tiles = (n_blocks + kOffsetsTile - 1) / kOffsetsTile;
+    launch_chained(batch_count_kernel<false>, dim3((unsigned int)n_units), dim3(kProjThreads), 0, st, vt, opt, ctrl,
+                   lb);
+    launch_chained(batch_offsets_kernel, dim3((unsigned int)(tiles > 0 ? tiles : 1)), dim3(kOffsetsThreads), 0, st,
+                   vt, ctrl, lb);
+    launch_chained(batch_project_kernel<false>, dim3((unsigned int)n_units), dim3(kProjThreads), kProjStageBytes, st,
+                   vt, opt, f, ctrl, (const unsigned long long*)lb);
 }
 
 /* Plain launches: one CTA per block (n_blocks known on the host).
