@@ -47,11 +47,11 @@ namespace lumen {
 constexpr int kGrad2D = 10;   /* cx, cy, ic00, ic01, ic11, opacity, r, g, b, depth */
 constexpr int kGrad2DStride = 12;   /* floats per Gaussian in splat2d: 16-byte rows for vector atomics */
 constexpr int kBwdChunk = kTilePixels;   /* instances staged per round */
-/* per warp: 32 rows of kGrad2D values (5 pairs), then zero padding up to
- * the last word a lane of the transposed read touches (2 * 31 + 60 * 5 + 1) */
+/* per warp: 32 rows of kGrad2D values, then zero padding up to the last
+ * word a lane of the transposed read touches (31 + 30 * 10) */
 constexpr int kRedRows = 32 * kGrad2D;
-constexpr int kRedWords = 364;
-constexpr int kRedReads = 6;
+constexpr int kRedWords = 360;
+constexpr int kRedReads = 11;
 
 struct BackwardSmem {
     float4 geo[kBwdChunk];        /* cx, cy, depth, opacity */
@@ -184,7 +184,6 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
         Gc = g_r * (out_rgb[pix * 3 + 0] - bg) + g_g * (out_rgb[pix * 3 + 1] - bg) +
              g_b * (out_rgb[pix * 3 + 2] - bg) + g_d * C_z - g_tail;
     }
-    const float2 G_rg = make_float2(g_r, g_g), G_bz = make_float2(g_b, g_d);
     /* the tile's sweep ends at the last instance any of its pixels visited */
     const int wlast = __reduce_max_sync(0xffffffffu, last);
     __syncthreads();
@@ -200,9 +199,8 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
         for (int t = 0; t < cnt; ++t) {
             const int j = s.list[warp][t];
             if (cs + j > wlast) break;   /* every pixel of the warp is past its last splat */
-            float2 g_xy = make_float2(0.0f, 0.0f), g_ac = make_float2(0.0f, 0.0f);
-            float2 g_rg = make_float2(0.0f, 0.0f), g_bz = make_float2(0.0f, 0.0f);
-            float gb = 0.0f, gop = 0.0f;
+            float gcx = 0.0f, gcy = 0.0f, ga = 0.0f, gb = 0.0f, gc = 0.0f, gop = 0.0f;
+            float gr = 0.0f, gg_ = 0.0f, gbl = 0.0f, gz = 0.0f;
             bool contrib = false;
             if (cs + j <= last) {
                 const float4 geo = s.geo[j], cc = s.con[j];
@@ -227,13 +225,11 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                         contrib = true;
                         const float4 col = s.col[j];
                         const float w = alpha * T;
-                        /* two-wide packed arithmetic: (r, g), (b, depth), (x, y) */
-                        const float2 ww = make_float2(w, w);
-                        g_rg = __fmul2_rn(G_rg, ww);
-                        g_bz = __fmul2_rn(G_bz, ww);
-                        const float2 gc2 = __ffma2_rn(G_bz, make_float2(col.z, geo.z),
-                                                      __fmul2_rn(G_rg, make_float2(col.x, col.y)));
-                        const float gcol = gc2.x + gc2.y;
+                        gr = g_r * w;
+                        gg_ = g_g * w;
+                        gbl = g_b * w;
+                        gz = g_d * w;
+                        const float gcol = g_r * col.x + g_g * col.y + g_b * col.z + g_d * geo.z;
                         GP += w * gcol;
                         const float one_minus = 1.0f - alpha;
                         const float dalpha = T * gcol - (Gc - GP) * fast_rcp(one_minus);
@@ -242,14 +238,13 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                             gop = dalpha * gexp;
                             if (!pclamp) {
                                 const float dpower = -gop * geo.w;
-                                const float2 d = make_float2(dx, dy);
-                                /* (0.5 dx^2, 0.5 dy^2) dpower and dx dy dpower */
-                                g_ac = __fmul2_rn(__fmul2_rn(d, d), make_float2(0.5f * dpower, 0.5f * dpower));
-                                gb = dx * dy * dpower;
+                                const float dxp = dx * dpower;
+                                ga = 0.5f * dx * dxp;
+                                gb = dy * dxp;
+                                gc = 0.5f * dy * dy * dpower;
                                 /* d dx / d cx = -1; the staged conic holds 0.5 a and 0.5 c */
-                                const float2 u = __ffma2_rn(make_float2(cc.y, 2.0f * cc.z), make_float2(dy, dy),
-                                                            __fmul2_rn(make_float2(2.0f * cc.x, cc.y), make_float2(dx, dx)));
-                                g_xy = __fmul2_rn(u, make_float2(-dpower, -dpower));
+                                gcx = -(2.0f * cc.x * dx + cc.y * dy) * dpower;
+                                gcy = -(cc.y * dx + 2.0f * cc.z * dy) * dpower;
                             }
                         }
                     }
@@ -257,36 +252,20 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
             }
             if (__any_sync(0xffffffffu, contrib)) {
                 /* warp sum by a shared-memory transpose: row `lane` holds this
-                 * lane's 10 values as 5 pairs; lane l < 30 adds pair l % 5 of
-                 * rows l / 5, l / 5 + 6, ... (packed adds), then two shuffle
-                 * steps combine the six partial sums of each pair */
+                 * lane's 10 values; lane l < 30 adds words l, l + 30, ...
+                 * (value l % 10 of rows l / 10, l / 10 + 3, ...) */
                 float2* row = reinterpret_cast<float2*>(red + lane * kGrad2D);
-                row[0] = g_xy;
-                row[1] = make_float2(g_ac.x, gb);
-                row[2] = make_float2(g_ac.y, gop);
-                row[3] = g_rg;
-                row[4] = g_bz;
+                row[0] = make_float2(gcx, gcy);
+                row[1] = make_float2(ga, gb);
+                row[2] = make_float2(gc, gop);
+                row[3] = make_float2(gr, gg_);
+                row[4] = make_float2(gbl, gz);
                 __syncwarp();
-                const float2* rd = reinterpret_cast<const float2*>(red) + lane;
-                float2 sum = rd[0];
+                float sum = 0.0f;
 #pragma unroll
-                for (int r = 1; r < kRedReads; ++r) sum = __fadd2_rn(sum, rd[30 * r]);
-                /* part q (lanes 5 q .. 5 q + 4): first q + (q + 3) for q < 3,
-                 * then lane p < 5 adds parts 1 and 2 of those sums */
-                float2 o, o2;
-                o.x = __shfl_down_sync(0xffffffffu, sum.x, 15);
-                o.y = __shfl_down_sync(0xffffffffu, sum.y, 15);
-                sum = __fadd2_rn(sum, o);
-                o.x = __shfl_down_sync(0xffffffffu, sum.x, 5);
-                o.y = __shfl_down_sync(0xffffffffu, sum.y, 5);
-                o2.x = __shfl_down_sync(0xffffffffu, sum.x, 10);
-                o2.y = __shfl_down_sync(0xffffffffu, sum.y, 10);
-                sum = __fadd2_rn(sum, __fadd2_rn(o, o2));
-                /* lane p < 5 holds values 2 p and 2 p + 1 */
-                if (lane < kGrad2D / 2) {
-                    if (sum.x != 0.0f) atomicAdd(&s.acc[j][2 * lane], sum.x);
-                    if (sum.y != 0.0f) atomicAdd(&s.acc[j][2 * lane + 1], sum.y);
-                }
+                for (int r = 0; r < kRedReads; ++r) sum += red[lane + 30 * r];
+                sum += __shfl_down_sync(0xffffffffu, sum, 10) + __shfl_down_sync(0xffffffffu, sum, 20);
+                if (lane < kGrad2D && sum != 0.0f) atomicAdd(&s.acc[j][lane], sum);
                 __syncwarp();
             }
         }
@@ -667,7 +646,7 @@ using namespace lumen;
 
 namespace lumen {
 
-/* Five 39.6 KB CTAs of the compositing adjoint per SM need the largest
+/* Five 39.4 KB CTAs of the compositing adjoint per SM need the largest
  * shared-memory carveout; set per device by configure_once. */
 void configure_backward_kernels() {
     cudaFuncSetAttribute(composite_backward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,

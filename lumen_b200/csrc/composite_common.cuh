@@ -45,27 +45,12 @@ __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float
     const float pcut = fminf(4.5f, __logf(op / min_alpha()) + 0.01f);
     if (pcut < 0.0f) return 0u;
     const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
-    /* the ellipse q <= qcut lies in |x| <= sqrt(qcut c / det), |y| <=
-     * sqrt(qcut a / det); blocks outside that box (widened by 0.1% and
-     * 0.01 px against rounding) are skipped before the exact test */
-    const float det_inv = __frcp_rn(a * c - b * b);
-    const float ex = sqrtf(qcut * c * det_inv) * 1.001f + 0.01f;
-    const float ey = sqrtf(qcut * a * det_inv) * 1.001f + 0.01f;
-    const float bx0 = tile_x0 + 0.5f - geo.x, by0 = tile_y0 + 0.5f - geo.y;
-    unsigned int box = 0;
-#pragma unroll
-    for (int w = 0; w < kTilePixels / 32; ++w) {
-        const float x0 = bx0 + (float)warp_block_x(w), y0 = by0 + (float)warp_block_y(w);
-        if (x0 <= ex && x0 + 7.0f >= -ex && y0 <= ey && y0 + 3.0f >= -ey) box |= 1u << w;
-    }
-    if (!box) return 0u;
     const float b_over_a = b * __frcp_rn(a), b_over_c = b * __frcp_rn(c);
     unsigned int m = 0;
 #pragma unroll
     for (int w = 0; w < kTilePixels / 32; ++w) {
-        if (!((box >> w) & 1u)) continue;
-        const float x0 = bx0 + (float)warp_block_x(w);
-        const float y0 = by0 + (float)warp_block_y(w);
+        const float x0 = tile_x0 + (float)warp_block_x(w) + 0.5f - geo.x;
+        const float y0 = tile_y0 + (float)warp_block_y(w) + 0.5f - geo.y;
         if (quad_min_rect(a, b, c, b_over_a, b_over_c, x0, x0 + 7.0f, y0, y0 + 3.0f) <= qcut) m |= 1u << w;
     }
     return m;
