@@ -40,8 +40,8 @@ UNIT = "frames/s"
 N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
 # DRAM bytes (read + write) of one composite_kernel<512> launch at the 1 M-Gaussian
-# 1080p workload, from an ncu capture (profiles/forward_config1_launches.md)
-COMPOSITE_DRAM_BYTES = 42.74e6
+# 1080p workload, from an ncu capture (profiles/forward_config1_kernels.md)
+COMPOSITE_DRAM_BYTES = 42.6e6
 def kernels_per_frame(n_tiles: int) -> int:
     """Kernels one forward frame launches: init, project, the depth sort's
     histogram and 4 digit passes, emit, the tile sort's histogram and one
@@ -1109,7 +1109,7 @@ def main():
                          "frac": achieved / hbm_peak, "traffic": COMPOSITE_DRAM_BYTES, "peak_source": peak_src,
                          "algorithmic_bytes": alg[dname],
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one composite_kernel "
-                                           "launch at this workload (profiles/forward_config1_launches.md)"},
+                                           "launch at this workload (profiles/forward_config1_kernels.md)"},
             "frame_roofline": {"bytes": b_fwd, "achieved": frame_gbs, "peak": hbm_peak, "unit": "GB/s",
                                "frac": frame_gbs / hbm_peak}}
     if not args.no_multiview:

@@ -132,7 +132,7 @@ __device__ __forceinline__ void blend_list(const CompositeSmem<kChunk>& s, int w
 
 /* One tile of the batch (batch-wide id gtile, owned by the last view whose
  * tile_begin <= gtile). */
-template <int kChunk>
+template <int kChunk, bool kTrack>
 __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const ViewTable* __restrict__ vt,
                                                const LumenSplatRecord* __restrict__ records, const LumenGpuFrame& f,
                                                long long capacity, Control* __restrict__ ctrl,
@@ -140,10 +140,9 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int view = n_views == 1 ? 0 : find_view_by_tile(vt, n_views, gtile);
     int tx, ty, px, py;
-    bool inside, any_instance, track;
+    bool inside, any_instance;
     {
         const ViewDesc& vd = vt->view[view];
-        track = vd.img.n_contrib != nullptr || vd.img.last_idx != nullptr;
         const int tiles_x = vd.tiles_x;
         const int tile = (int)(gtile - vd.tile_begin);
         tx = tile % tiles_x;
@@ -224,22 +223,12 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
                 cnt = (cnt + kVoteGroup - 1) & ~(kVoteGroup - 1);
                 __syncwarp();
                 PixelState px_state{T, cr, cg, cb, dep, acc, count, last, done};
-                if (track) {
-                    if (clamp) {
-                        if (mode_alpha) blend_list<kChunk, true, true, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                        else blend_list<kChunk, true, false, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                    } else {
-                        if (mode_alpha) blend_list<kChunk, false, true, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                        else blend_list<kChunk, false, false, true>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                    }
+                if (clamp) {
+                    if (mode_alpha) blend_list<kChunk, true, true, kTrack>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    else blend_list<kChunk, true, false, kTrack>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
                 } else {
-                    if (clamp) {
-                        if (mode_alpha) blend_list<kChunk, true, true, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                        else blend_list<kChunk, true, false, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                    } else {
-                        if (mode_alpha) blend_list<kChunk, false, true, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                        else blend_list<kChunk, false, false, false>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
-                    }
+                    if (mode_alpha) blend_list<kChunk, false, true, kTrack>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
+                    else blend_list<kChunk, false, false, kTrack>(s, warp, cnt, cs, pxc, pyc, thr, px_state);
                 }
                 T = px_state.T; cr = px_state.cr; cg = px_state.cg; cb = px_state.cb; dep = px_state.dep;
                 acc = px_state.acc; count = px_state.count; last = px_state.last; done = px_state.done;
@@ -274,8 +263,9 @@ __device__ __forceinline__ void composite_tile(CompositeSmem<kChunk>& s, const V
     if (img.last_idx) img.last_idx[pix] = last;
 }
 
-/* One CTA per tile of the batch. */
-template <int kChunk>
+/* One CTA per tile of the batch. kTrack: keep contributor counts and
+ * last-visited offsets (some view's image asks for them). */
+template <int kChunk, bool kTrack>
 __global__ void __launch_bounds__(kTilePixels, kCompositeBlocksPerSm)
 composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplatRecord* __restrict__ records,
                  LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt,
@@ -283,12 +273,12 @@ composite_kernel(const ViewTable* __restrict__ vt, int n_views, const LumenSplat
     chain_begin();
     __shared__ CompositeSmem<kChunk> s;
     init_padding_splat(s);
-    composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, tile_offset + blockIdx.x);
+    composite_tile<kChunk, kTrack>(s, vt, records, f, capacity, ctrl, opt, n_views, tile_offset + blockIdx.x);
 }
 
 /* Persistent form for a grid fixed in advance (a captured graph replayed
  * for batches of any size): CTAs take tiles in ticket order. */
-template <int kChunk>
+template <int kChunk, bool kTrack>
 __global__ void __launch_bounds__(kTilePixels, kCompositeBlocksPerSm)
 composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRecord* __restrict__ records,
                             LumenGpuFrame f, long long capacity, Control* __restrict__ ctrl, LumenRenderOptions opt) {
@@ -302,40 +292,56 @@ composite_persistent_kernel(const ViewTable* __restrict__ vt, const LumenSplatRe
         __syncthreads();
         const long long t = s.ticket;
         if (t >= total) break;
-        composite_tile(s, vt, records, f, capacity, ctrl, opt, n_views, t);
+        composite_tile<kChunk, kTrack>(s, vt, records, f, capacity, ctrl, opt, n_views, t);
         __syncthreads();
     }
 }
 
-template <int kChunk>
+template <int kChunk, bool kTrack>
 static void launch_composite_chunk(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
                                    const LumenRenderOptions& opt, long long tile_offset, long long n_tiles,
                                    bool persistent, int num_sms, cudaStream_t st) {
     if (persistent) {
-        launch_chained(composite_persistent_kernel<kChunk>, dim3(kCompositeBlocksPerSm * num_sms), dim3(kTilePixels), 0, st, vt,
-                       (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt);
+        launch_chained(composite_persistent_kernel<kChunk, kTrack>, dim3(kCompositeBlocksPerSm * num_sms),
+                       dim3(kTilePixels), 0, st, vt, (const LumenSplatRecord*)f.records, f,
+                       (long long)f.instance_capacity, ctrl, opt);
     } else {
-        launch_chained(composite_kernel<kChunk>, dim3((unsigned int)n_tiles), dim3(kTilePixels), 0, st, vt, n_views,
-                       (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt, tile_offset);
+        launch_chained(composite_kernel<kChunk, kTrack>, dim3((unsigned int)n_tiles), dim3(kTilePixels), 0, st, vt,
+                       n_views, (const LumenSplatRecord*)f.records, f, (long long)f.instance_capacity, ctrl, opt,
+                       tile_offset);
     }
+}
+
+template <int kChunk>
+static void launch_composite_track(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
+                                   const LumenRenderOptions& opt, long long tile_offset, long long n_tiles,
+                                   bool persistent, bool track, int num_sms, cudaStream_t st) {
+    if (track)
+        launch_composite_chunk<kChunk, true>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+    else
+        launch_composite_chunk<kChunk, false>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
 }
 
 /* chunk: instances staged per round, one of kCompositeChunks. Plain
  * launches shade tiles [tile_offset, tile_offset + n_tiles) of the batch;
- * persistent launches take every tile of the table by ticket. */
+ * persistent launches take every tile of the table by ticket. track: some
+ * view's image asks for contributor counts or last-visited offsets. */
 void launch_composite(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
                       const LumenRenderOptions& opt, long long tile_offset, long long n_tiles, bool persistent,
-                      int chunk, int num_sms, cudaStream_t st) {
+                      int chunk, bool track, int num_sms, cudaStream_t st) {
     if (n_tiles <= 0) return;
     switch (chunk) {
         case 128:
-            launch_composite_chunk<128>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+            launch_composite_track<128>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, track, num_sms,
+                                        st);
             break;
         case 512:
-            launch_composite_chunk<512>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+            launch_composite_track<512>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, track, num_sms,
+                                        st);
             break;
         default:
-            launch_composite_chunk<256>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, num_sms, st);
+            launch_composite_track<256>(vt, n_views, f, ctrl, opt, tile_offset, n_tiles, persistent, track, num_sms,
+                                        st);
             break;
     }
 }

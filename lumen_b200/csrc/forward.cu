@@ -47,7 +47,7 @@ void launch_sorted_keys64(const LumenGpuFrame& f, const Control* ctrl, int key_m
                           int num_sms, cudaStream_t st);
 void launch_composite(const ViewTable* vt, int n_views, const LumenGpuFrame& f, Control* ctrl,
                       const LumenRenderOptions& opt, long long tile_offset, long long n_tiles, bool persistent,
-                      int chunk, int num_sms, cudaStream_t st);
+                      int chunk, bool track, int num_sms, cudaStream_t st);
 void configure_sort_kernels();
 
 int device_sm_count() {
@@ -208,7 +208,7 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
     launch_ranges(f, ctrl, vt, sms, s);
     if (ev) cudaEventRecord(ev[3], s);
     if (!with_composite) return;
-    launch_composite(vt, n_views, f, ctrl, opt, 0, n_tiles, persistent, lc.composite_chunk, sms, s);
+    launch_composite(vt, n_views, f, ctrl, opt, 0, n_tiles, persistent, lc.composite_chunk, lc.track != 0, sms, s);
     if (ev) cudaEventRecord(ev[4], s);
 }
 
@@ -254,8 +254,9 @@ static void single_view_table(const LumenGpuGaussians* g, const LumenViewCamera*
 
 static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamera* cam, const LumenRenderOptions* opt,
                                 LumenGpuFrame* f, LumenGpuImage* img, cudaEvent_t* ev, void* stream,
-                                const LaunchConfig& lc = kDefaultLaunch) {
+                                LaunchConfig lc = kDefaultLaunch) {
     if (!launch_ok(lc)) return LUMEN_ERROR_INVALID_ARGUMENT;
+    if (img) lc.track = img->n_contrib || img->last_idx;
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
     if (!img || (!img->rgb && !img->rgb8) || !frame_ok(f, g->count, true)) return LUMEN_ERROR_INVALID_ARGUMENT;
@@ -306,7 +307,7 @@ LumenStatus forward_banded(const LumenGpuGaussians* g, const LumenViewCamera* ca
     for (int b = 0; b < n_bands; ++b) {
         const int r0 = (int)((long long)tiles_y * b / n_bands), r1 = (int)((long long)tiles_y * (b + 1) / n_bands);
         launch_composite(vt, 1, *f, ctrl, *opt, (long long)r0 * tiles_x, (long long)(r1 - r0) * tiles_x, false,
-                         kDefaultLaunch.composite_chunk, sms, s);
+                         kDefaultLaunch.composite_chunk, img->n_contrib || img->last_idx, sms, s);
         const int y0 = r0 * kTile, y1 = r1 * kTile < cam->height ? r1 * kTile : cam->height;
         if (after_band) after_band(ctx, y0, y1, s);
     }
@@ -374,8 +375,11 @@ static LumenStatus batch_impl(const LumenGpuBatchView* views, int n_views, const
     cudaError_t e = cudaMemcpyAsync(base + L.table_off, host.data(), host.size(), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return map_cuda(e);
     launch_init(L, base, nullptr, nullptr, s);
-    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, kDefaultLaunch, ev, s, true,
-                    hdr.total_units);
+    LaunchConfig lc = kDefaultLaunch;
+    lc.track = 0;
+    for (int v = 0; v < n_views; ++v)
+        if (views[v].image.n_contrib || views[v].image.last_idx) lc.track = 1;
+    launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, lc, ev, s, true, hdr.total_units);
     return map_cuda(cudaGetLastError());
 }
 
@@ -406,7 +410,7 @@ LumenStatus lumen_gpu_render_forward_ex(const LumenGpuGaussians* g, const LumenV
                                         const LumenRenderOptions* opt, const LumenGpuLaunch* launch,
                                         LumenGpuFrame* f, LumenGpuImage* img, LumenGpuStageTimer* t, void* stream) {
     if (!launch) return LUMEN_ERROR_INVALID_ARGUMENT;
-    const LaunchConfig lc = {launch->composite_chunk, launch->depth_sort_items, launch->tile_sort_items};
+    const LaunchConfig lc = {launch->composite_chunk, launch->depth_sort_items, launch->tile_sort_items, 1};
     if (!t) return forward_impl(g, cam, opt, f, img, nullptr, stream, lc);
     if (t->next >= t->max_frames) return LUMEN_ERROR_INVALID_ARGUMENT;
     LumenStatus st = forward_impl(g, cam, opt, f, img, t->ev + (size_t)t->next * 5, stream, lc);

@@ -356,8 +356,8 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
 
 constexpr int kCamWords = (int)(sizeof(DevCamera) / 4);
 static_assert(sizeof(DevCamera) % 4 == 0 && kCamWords <= kProjThreads, "camera copy layout");
-constexpr int kOffsetsThreads = 256;
-constexpr int kOffsetsItems = 32;   /* 8192 counts per tile: one tile for a 1M-Gaussian view */
+constexpr int kOffsetsThreads = 1024;
+constexpr int kOffsetsItems = 8;    /* 8192 counts per tile: one tile for a 1M-Gaussian view */
 constexpr int kOffsetsTile = kOffsetsThreads * kOffsetsItems;
 /* resident projection CTAs per SM: 64 registers, 8 x 24.6 KB of staged SH rows */
 constexpr int kBatchProjectCtas = 8;
