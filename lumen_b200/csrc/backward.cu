@@ -552,7 +552,7 @@ __device__ __forceinline__ void project_backward_gaussian(const LumenGpuGaussian
  * asynchronous 16-byte copies (swizzled rows, see sh_swizzle), each thread
  * forms its Gaussian's gradients (its dL/dsh in place of its row), and the
  * rows go out with coalesced 16-byte stores. Culled Gaussians get zeros. */
-__global__ void __launch_bounds__(kProjBwdThreads, 6)
+__global__ void __launch_bounds__(kProjBwdThreads, 8)
 project_backward_kernel(LumenGpuGaussians g, LumenViewCamera camera, LumenRenderOptions opt,
                         const int* __restrict__ radii, const float* __restrict__ grad2d, LumenGpuGradients out) {
     chain_begin();

@@ -4,8 +4,10 @@
  * timing, and a renderer that owns and grows its frame buffers.
  *
  * Launch sequence of a frame (all on the caller's stream, no host sync):
- *   memset(control + both look-back scans)
- *   project            K1: projection, cull, SH, compacting scan, depth keys
+ *   frame_init         control block and look-back descriptors zeroed, view table
+ *   batch_count        K1a: each block's visible count (geometry only)
+ *   batch_offsets      K1b: the counts scanned into each block's first visible index
+ *   batch_project      K1c: projection, cull, SH, records and depth keys at those offsets
  *   histogram<u32>     depth-key digits of the visible splats
  *   onesweep_pass x4   stable sort of visible splats by depth key
  *   emit               K2: (tile id, visible index) per covered tile, in depth order
@@ -191,7 +193,7 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
         if (ev) cudaEventRecord(ev[1], s);
         launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
                       &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,
-                      lc.depth_sort_items, lc.depth_key_bytes > 0 ? lc.depth_key_bytes : 4, sms, s);
+                      lc.depth_sort_items, 4, sms, s);
         launch_emit(vt, f, ctrl, emit_lb, L.proj_blocks, persistent, sms, s);
     } else if (ev) {
         cudaEventRecord(ev[1], s);
@@ -257,7 +259,6 @@ static LumenStatus forward_impl(const LumenGpuGaussians* g, const LumenViewCamer
                                 LaunchConfig lc = kDefaultLaunch) {
     if (!launch_ok(lc)) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (img) lc.track = img->n_contrib || img->last_idx;
-    if (cam && opt) lc.depth_key_bytes = depth_key_bytes_for(*cam, opt->key_mode);
     LumenStatus st = check_inputs(g, cam, opt);
     if (st != LUMEN_SUCCESS) return st;
     if (!img || (!img->rgb && !img->rgb8) || !frame_ok(f, g->count, true)) return LUMEN_ERROR_INVALID_ARGUMENT;
@@ -299,9 +300,8 @@ LumenStatus forward_banded(const LumenGpuGaussians* g, const LumenViewCamera* ca
     ViewDesc v{};
     single_view_table(g, cam, img, L, tiles, &hdr, &v);
     launch_init(L, base, &hdr, &v, s);
-    LaunchConfig lc = kDefaultLaunch;
-    lc.depth_key_bytes = depth_key_bytes_for(*cam, opt->key_mode);
-    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, lc, nullptr, s, false, hdr.total_units);
+    launch_pipeline(L, base, *opt, *f, g->count, tiles, 1, false, kDefaultLaunch, nullptr, s, false,
+                    hdr.total_units);
     Control* ctrl = (Control*)(base + L.control_off);
     const ViewTable* vt = (const ViewTable*)(base + L.table_off);
     const int sms = device_sm_count();
@@ -379,12 +379,8 @@ static LumenStatus batch_impl(const LumenGpuBatchView* views, int n_views, const
     launch_init(L, base, nullptr, nullptr, s);
     LaunchConfig lc = kDefaultLaunch;
     lc.track = 0;
-    lc.depth_key_bytes = 1;
-    for (int v = 0; v < n_views; ++v) {
+    for (int v = 0; v < n_views; ++v)
         if (views[v].image.n_contrib || views[v].image.last_idx) lc.track = 1;
-        const int db = depth_key_bytes_for(views[v].camera, opt->key_mode);
-        if (db > lc.depth_key_bytes) lc.depth_key_bytes = db;
-    }
     launch_pipeline(L, base, *opt, *f, slots, hdr.total_tiles, n_views, false, lc, ev, s, true, hdr.total_units);
     return map_cuda(cudaGetLastError());
 }
@@ -416,7 +412,7 @@ LumenStatus lumen_gpu_render_forward_ex(const LumenGpuGaussians* g, const LumenV
                                         const LumenRenderOptions* opt, const LumenGpuLaunch* launch,
                                         LumenGpuFrame* f, LumenGpuImage* img, LumenGpuStageTimer* t, void* stream) {
     if (!launch) return LUMEN_ERROR_INVALID_ARGUMENT;
-    const LaunchConfig lc = {launch->composite_chunk, launch->depth_sort_items, launch->tile_sort_items, 1, 0};
+    const LaunchConfig lc = {launch->composite_chunk, launch->depth_sort_items, launch->tile_sort_items, 1};
     if (!t) return forward_impl(g, cam, opt, f, img, nullptr, stream, lc);
     if (t->next >= t->max_frames) return LUMEN_ERROR_INVALID_ARGUMENT;
     LumenStatus st = forward_impl(g, cam, opt, f, img, t->ev + (size_t)t->next * 5, stream, lc);

@@ -306,10 +306,7 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
                     f.vals[0][pos] = s.vis[lo];
                 }
             }
-            /* the owner slots are reused by the next window; after the last
-             * one, the barrier below the key-range reduction keeps the next
-             * block's staging behind every thread's writes */
-            if (a + kEmitWindow < block_inst) __syncthreads();
+            __syncthreads();
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

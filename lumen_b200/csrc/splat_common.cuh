@@ -73,27 +73,12 @@ struct LaunchConfig {
     int tile_sort_items;   /* keys per thread in a tile-sort digit pass: 8 or 16 */
     int track;             /* 1: some view's image asks for contributor counts or last-visited
                               offsets (the compositor then keeps them); set by the host */
-    int depth_key_bytes;   /* low bytes of the depth keys that can vary (0: all 4); set by the host */
 };
-
-/* Depth-key bytes that can vary for a camera: millimetre keys never exceed
- * the far plane's key (z <= far after culling, and z * 1000 rounds
- * monotonically), so a frame whose far plane is at most 16.7 km needs three
- * digit passes; float-bit keys need four. */
-inline int depth_key_bytes_for(const LumenViewCamera& cam, int key_mode) {
-    if (key_mode != 0) return 4;
-    const float far_key = cam.far_plane * 1000.0f;
-    if (!(far_key >= 0.0f) || far_key >= 2147483647.0f) return 4;
-    long long k = (long long)far_key + 1;
-    int bytes = 0;
-    while (k > 0) { ++bytes; k >>= 8; }
-    return bytes < 1 ? 1 : bytes;
-}
 /* measured on B200 at 1080p with 1 M Gaussians: 512-instance compositor
  * chunks (0.233 against 0.238 ms for 256, 0.259 for 128); 2048-key tiles
  * shorten the (smaller) depth sort, 4096-key tiles suit the tile sort
  * (0.234 ms against 0.256 for 2048 and 0.243 for 6144) */
-constexpr LaunchConfig kDefaultLaunch = {512, 8, 16, 1, 0};
+constexpr LaunchConfig kDefaultLaunch = {512, 8, 16, 1};
 
 __host__ __device__ constexpr inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
