@@ -55,7 +55,7 @@ constexpr int kRedReads = 11;
 
 struct BackwardSmem {
     float4 geo[kBwdChunk];        /* cx, cy, depth, opacity */
-    float4 con[kBwdChunk];        /* 0.5 ic00, ic01, 0.5 ic11, - (the forward's prescaled conic) */
+    float4 con[kBwdChunk];        /* 0.5 ic00, ic01, 0.5 ic11 (the forward's prescaled conic), power cutoff */
     float4 col[kBwdChunk];        /* r, g, b, - */
     unsigned char mask[kBwdChunk];
     unsigned short list[kTilePixels / 32][kBwdChunk];
@@ -89,7 +89,7 @@ __device__ __forceinline__ int stage_chunk(BackwardSmem& s, const LumenSplatReco
             const float4* r4 = reinterpret_cast<const float4*>(records + v);
             const float4 geo = __ldg(r4), con = __ldg(r4 + 1);
             s.geo[tid] = geo;
-            s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, 0.0f);
+            s.con[tid] = make_float4(0.5f * con.x, con.y, 0.5f * con.z, splat_power_cutoff(geo.w));
             s.col[tid] = __ldg(r4 + 2);
             s.gid[tid] = visible_ids[v];
             m = reach_mask(geo, con, tile_x0, tile_y0);
@@ -210,7 +210,7 @@ composite_backward_kernel(const LumenSplatRecord* __restrict__ records, LumenGpu
                                         __fmul_rn(__fmul_rn(cc.z, dy), dy));
                 bool pclamp = false;
                 if (power < 0.0f) { power = 0.0f; pclamp = true; }
-                if (!(power > 4.5f)) {
+                if (!(power > cc.w)) {   /* beyond 4.5, or certain to fall below 1/255 */
                     float gexp = fast_exp_neg(power);
                     float raw = geo.w * gexp;
                     /* near the 1/255 skip or the 0.99 clamp the decision is taken

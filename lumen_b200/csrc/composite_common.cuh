@@ -32,6 +32,17 @@ __device__ __forceinline__ float quad_min_rect(float a, float b, float c, float 
     return m;
 }
 
+/* The power above which a splat cannot be blended at any pixel: the
+ * reference skips power > 4.5 (compositor.mojo:80-82), and alpha =
+ * opacity * exp(-power) falls below the 1/255 skip (compositor.mojo:33-35)
+ * once power exceeds ln(opacity / (1/255)); the 1e-3 margin is far above
+ * the rounding of the exponential and the logarithm, so a pixel beyond the
+ * cutoff is one the exact test skips too (and one at or below it takes the
+ * exact test). */
+__device__ __forceinline__ float splat_power_cutoff(float opacity) {
+    return fminf(4.5f, logf(opacity / min_alpha()) + 1e-3f);
+}
+
 /* Bit w set when the splat may reach the blend threshold at some pixel
  * centre of warp w's block. A pixel is blended only if
  * power <= 4.5 and opacity * exp(-power) >= 1/255 (compositor.mojo:62-89,
