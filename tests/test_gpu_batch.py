@@ -140,3 +140,32 @@ def test_config2_shape_batch():
                 a, c = getattr(b.images[v], name), getattr(s, name)
                 assert torch.equal(a, c), f"view {v}: {name} differs"
     assert b.n_instances == total
+
+
+@pytest.mark.parametrize("term_mode", [0, 1])
+def test_interleaved_scene_groups(term_mode):
+    """Views of one scene scattered among views of others (A B A C B A C),
+    the order a server queue gives: the Gaussian-major projection groups the
+    views of each scene wherever they sit in the batch, and every view still
+    equals its standalone render."""
+    a = device_scene(scenes.box_scene(6_000, seed=31))
+    b = device_scene(scenes.box_scene(2_500, seed=32))
+    c = device_scene(scenes.box_scene(9_000, seed=33, centre=(0, 0, 4)))
+    ca = scenes.orbit_cameras(3, 160, 96, radius=9.0)
+    cb = scenes.orbit_cameras(2, 123, 77, radius=7.0)
+    cc = scenes.orbit_cameras(2, 256, 144, radius=11.0, centre=(0, 0, 4))
+    views = [(a, ca[0]), (b, cb[0]), (a, ca[1]), (c, cc[0]), (b, cb[1]), (a, ca[2]), (c, cc[1])]
+    check_views_against_single(views, RenderOptions(term_mode=term_mode))
+
+
+def test_same_scene_storage_with_different_counts_is_not_grouped():
+    """Two scenes sharing parameter storage but with different Gaussian
+    counts (a prefix of the arrays) are different groups: each view equals
+    its standalone render."""
+    from lumen_b200 import render as R
+    full = device_scene(scenes.box_scene(5_000, seed=34))
+    t = full.tensors
+    prefix = R.Scene(t[0][:3_000], t[1][:3_000], t[2][:3_000], t[3][:3_000], t[4][:3_000])
+    cams = scenes.orbit_cameras(4, 144, 96, radius=9.0)
+    views = [(full, cams[0]), (prefix, cams[1]), (full, cams[2]), (prefix, cams[3])]
+    check_views_against_single(views, RenderOptions(term_mode=1))
