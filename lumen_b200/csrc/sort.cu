@@ -14,9 +14,9 @@
  *    leaves a stable sort unchanged, so it is skipped on the device.
  *  - each digit pass is one persistent kernel: a CTA takes 4096-key tiles in
  *    ticket order, counts the tile's digits and publishes the counts at
- *    once, ranks its keys with a warp-level multisplit (one ballot per
- *    varying bit of the digit; stable: warp order, then item order, then
- *    lane order) straight into shared memory, and then resolves the global
+ *    once, ranks its keys with a warp-level multisplit (a shared match mask
+ *    per digit; stable: warp order, then item order, then lane order)
+ *    straight into shared memory, and then resolves the global
  *    digit offsets by decoupled look-back over earlier tiles. Keys are
  *    written out in digit runs.
  *  - every wait on another CTA's descriptor is bounded.
@@ -133,6 +133,7 @@ struct PassSmem {
     KeyT keys[kSortThreads * kItems];
     unsigned int vals[kSortThreads * kItems];
     unsigned int whist[kSortThreads / 32][256];
+    unsigned int match[2][kSortThreads / 32][256];   /* per item parity and warp: lanes holding each digit */
     unsigned int digit_start[256];
     long long gbase[256];
     unsigned int goffset[256];
@@ -221,9 +222,8 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         __syncthreads();
     }
 
-    /* the bits of this digit that vary over the keys (the others are equal
-     * in every key and need no ballot) */
-    const unsigned int dbits = (unsigned int)(((sc->key_or & sc->key_or_not) >> shift) & 0xFFull);
+    /* the match masks start clear; each item's leaders clear what it set */
+    for (int j = tid; j < 2 * (kSortThreads / 32) * 256; j += kSortThreads) (&s.match[0][0][0])[j] = 0u;
 
     for (;;) {
         if (tid == 0) s.tile = atomicAdd(&sc->pass_ticket[digit], 1u);
@@ -279,29 +279,32 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
         }
         __syncthreads();
         /* warp-level stable multisplit (warp order, then item order, then
-         * lane order): the lanes holding the same digit are found with one
-         * ballot per varying bit, a constant cost where a match instruction
-         * slows down with the number of distinct digits in the warp. The
-         * warp's running count of each digit starts at its warp-exclusive
-         * offset, so a key's rank is its place in the tile's digit run and it
-         * goes straight to its slot in shared memory. */
+         * lane order): each lane sets its bit in the shared mask of its
+         * digit, so after a warp barrier the mask names the lanes holding the
+         * same digit (one shared atomic per key, where a ballot per digit bit
+         * costs eight vote and select steps and a match instruction slows
+         * down with the number of distinct digits). The lowest such lane
+         * advances the warp's running count of the digit, which starts at its
+         * warp-exclusive offset, and clears the mask; a key's rank is then its
+         * place in the tile's digit run and it goes straight to its slot in
+         * shared memory. Items alternate between two mask sets, so the
+         * clearing of one item's masks needs no barrier of its own before the
+         * next item sets the other set. */
 #pragma unroll
         for (int it = 0; it < kItems; ++it) {
             const bool valid = wbase + it * 32 + lane < K;
             const unsigned int d = (unsigned int)((k[it] >> shift) & 0xFF);
-            unsigned int peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                if (!((dbits >> b) & 1u)) continue;
-                const unsigned int bit = (d >> b) & 1u;
-                const unsigned int bal = __ballot_sync(0xffffffffu, bit);
-                peers &= bit ? bal : ~bal;
-            }
+            unsigned int* mk = s.match[it & 1][warp];
+            if (valid) atomicOr(&mk[d], 1u << lane);
+            __syncwarp();
+            const unsigned int peers = valid ? mk[d] : 0u;
             unsigned int prior = 0;
             if (valid) prior = s.whist[warp][d];
             __syncwarp();
-            if (valid && lane == __ffs(peers) - 1) s.whist[warp][d] = prior + __popc(peers);
-            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1) {
+                s.whist[warp][d] = prior + __popc(peers);
+                mk[d] = 0u;
+            }
             if (valid) {
                 const unsigned int pos = s.digit_start[d] + prior + __popc(peers & lanemask_lt());
                 s.keys[pos] = k[it];
