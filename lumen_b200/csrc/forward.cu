@@ -35,7 +35,11 @@ void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& 
                     Control* ctrl, unsigned long long* lb, long long n_blocks, bool persistent, int num_sms,
                     cudaStream_t st);
 void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb,
-                 long long n_blocks, bool persistent, int num_sms, cudaStream_t st);
+                 unsigned int* sort_lb, long long sort_lb_tiles, int sort_tile_keys, long long n_blocks,
+                 bool persistent, int num_sms, cudaStream_t st);
+void launch_tile_sort_counted(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1,
+                              long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap,
+                              unsigned int* err, int items, int key_bytes, int num_sms, cudaStream_t st);
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
                    SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
                    const long long* n_range_tiles, unsigned int* err, int items, int key_bytes, int num_sms,
@@ -194,18 +198,26 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
         launch_sort32(f.depth_keys[0], f.depth_order[0], f.depth_keys[1], f.depth_order[1], n_slots,
                       &ctrl->depth_sort, depth_lb, L.depth_tiles, nullptr, nullptr, &ctrl->error_flags,
                       lc.depth_sort_items, 4, sms, s);
-        launch_emit(vt, f, ctrl, emit_lb, L.proj_blocks, persistent, sms, s);
+        launch_emit(vt, f, ctrl, emit_lb, tile_lb, 2 * L.sort_tiles, kSortThreads * lc.tile_sort_items,
+                    L.proj_blocks, persistent, sms, s);
     } else if (ev) {
         cudaEventRecord(ev[1], s);
     }
     /* the tile-sort region holds 4 passes of 2048-key tiles; tile ids below
      * n_tiles (the batch's, or the bound a persistent launch is sized for)
-     * vary in their low ceil(log2(n_tiles) / 8) bytes only */
+     * vary in their low ceil(log2(n_tiles) / 8) bytes only. After an
+     * emission the digit counts, look-back tiles and ranges are ready;
+     * without one (no Gaussians) the sort's histogram kernel does that. */
     int tile_bytes = 0;
     for (long long t = n_tiles - 1; t > 0; t >>= 8) ++tile_bytes;
-    launch_sort32(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort, tile_lb,
-                  2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.tile_sort_items,
-                  tile_bytes, sms, s);
+    if (n_slots > 0)
+        launch_tile_sort_counted(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort,
+                                 tile_lb, 2 * L.sort_tiles, &ctrl->error_flags, lc.tile_sort_items, tile_bytes, sms,
+                                 s);
+    else
+        launch_sort32(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort, tile_lb,
+                      2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.tile_sort_items,
+                      tile_bytes, sms, s);
     if (ev) cudaEventRecord(ev[2], s);
     launch_ranges(f, ctrl, vt, sms, s);
     if (ev) cudaEventRecord(ev[3], s);

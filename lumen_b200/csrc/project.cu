@@ -172,13 +172,13 @@ project_kernel(const ViewTable* __restrict__ vt, int n_views_hint, LumenRenderOp
     }
 }
 
-/* Instances of an emission block resolved to their splats per window. */
-constexpr int kEmitWindow = 2048;
-constexpr int kEmitPerThread = kEmitWindow / kEmitThreads;
-static_assert(kEmitPerThread == 8, "two 16-byte slot groups per thread");
+/* Instances of an emission warp resolved to their splats per window. */
+constexpr int kEmitWindow = 256;
+constexpr int kEmitPerLane = kEmitWindow / 32;
+static_assert(kEmitPerLane == 8, "two 16-byte slot groups per lane");
 
 struct EmitSmem {
-    __align__(16) unsigned int owner[kEmitWindow];   /* 1 + the block-local splat of each window slot */
+    __align__(16) unsigned int owner[kEmitThreads / 32][kEmitWindow];   /* 1 + the warp lane of each window slot */
     unsigned int blk;
     unsigned int warp_tot[kEmitThreads / 32];
     unsigned long long inst_base;
@@ -189,26 +189,44 @@ struct EmitSmem {
     unsigned int tile_base[kEmitThreads]; /* batch-wide id of the view's tile 0 */
     unsigned int tiles_x[kEmitThreads];
     float rcp_width[kEmitThreads];        /* 1 / width, for the row of an instance */
+    unsigned int hist[3][256];            /* the block's tile ids: counts of each digit value */
     unsigned long long key_or, key_or_not;
 };
 
 /* Like project_kernel: 256 consecutive splats of the depth order per ticket.
- * Tile ids are batch-wide (view tile_begin + ty * tiles_x + tx). */
+ * Tile ids are batch-wide (view tile_begin + ty * tiles_x + tx).
+ *
+ * The emission also does the tile sort's preparation, so that the sort
+ * needs no pass of its own over the instances: it counts the digit values
+ * of the tile ids it writes (per block in shared memory, then added to the
+ * sort's histogram), clears the sort's look-back descriptors of the
+ * 256 * sort_items-key tiles that start among its instances, and fills the
+ * tile ranges with (-1, -1). */
 template <bool kPersistent>
 __global__ void __launch_bounds__(kEmitThreads)
-emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, unsigned long long* lb) {
+emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, unsigned long long* lb,
+            unsigned int* sort_lb, long long sort_lb_tiles, int sort_tile_keys) {
     chain_begin();
     __shared__ EmitSmem s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long V = ctrl->n_visible;
     const unsigned int* order = ctrl->depth_sort.sorted_buffer ? f.depth_order[1] : f.depth_order[0];
     const long long cap = f.instance_capacity;
+    /* the tile-id bytes that can vary: ids are below the batch's tile count */
+    const long long n_tiles = vt->hdr.total_tiles;
+    int nd = 0;
+    for (long long t = n_tiles - 1; t > 0 && nd < 3; t >>= 8) ++nd;
+    {
+        const long long nthreads = (long long)gridDim.x * blockDim.x;
+        for (long long j = (long long)blockIdx.x * blockDim.x + tid; j < 2 * n_tiles; j += nthreads) f.ranges[j] = -1;
+    }
     for (;;) {
         if (tid == 0) {
             s.blk = atomicAdd(&ctrl->emit_ticket, 1u);
             s.key_or = 0ull;
             s.key_or_not = 0ull;
         }
+        for (int d = 0; d < nd; ++d) s.hist[d][tid] = 0u;
         __syncthreads();
         const int blk = (int)s.blk;
         if ((long long)blk * kEmitThreads >= V) break;   /* past the visible splats: no look-back waits on it */
@@ -243,26 +261,31 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         __syncthreads();
         const unsigned long long inst_base = s.inst_base;
         unsigned int kor = 0u, knot = 0u;
-        /* The block's instances, kEmitWindow at a time. Each splat marks the
-         * slot where its run of instances enters the window (the splat
+        /* The warp's instances (those of its 32 splats, consecutive in the
+         * block's instance order), kEmitWindow at a time. Each splat marks
+         * the slot where its run of instances enters the window (the splat
          * already running at the window's start marks slot 0); a prefix
          * maximum over the marks then gives every slot its splat without a
-         * search, and consecutive threads write consecutive instances. */
+         * search, and consecutive lanes write consecutive instances. Warps
+         * work through their windows independently: only warp barriers. */
         const unsigned int my_end = excl + cnt;
-        for (unsigned int a = 0; a < block_inst; a += kEmitWindow) {
-            uint4* o4 = reinterpret_cast<uint4*>(s.owner) + tid * 2;
+        const unsigned int w_begin = __shfl_sync(0xffffffffu, excl, 0);
+        const unsigned int w_end = __shfl_sync(0xffffffffu, my_end, 31);
+        unsigned int* own = s.owner[warp];
+        uint4* o4 = reinterpret_cast<uint4*>(own) + lane * 2;
+        for (unsigned int a = w_begin; a < w_end; a += kEmitWindow) {
             o4[0] = make_uint4(0u, 0u, 0u, 0u);
             o4[1] = make_uint4(0u, 0u, 0u, 0u);
-            __syncthreads();
-            if (cnt && my_end > a && excl < a + kEmitWindow) s.owner[(excl > a ? excl : a) - a] = (unsigned int)tid + 1u;
-            __syncthreads();
-            /* inclusive prefix maximum: eight consecutive slots per thread,
-             * then across threads */
+            __syncwarp();
+            if (cnt && my_end > a && excl < a + kEmitWindow) own[(excl > a ? excl : a) - a] = (unsigned int)lane + 1u;
+            __syncwarp();
+            /* inclusive prefix maximum: eight consecutive slots per lane,
+             * then across the lanes */
             const uint4 g0 = o4[0], g1 = o4[1];
-            unsigned int m[kEmitPerThread] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+            unsigned int m[kEmitPerLane] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
 #pragma unroll
-            for (int k = 1; k < kEmitPerThread; ++k) m[k] = max(m[k], m[k - 1]);
-            unsigned int x = m[kEmitPerThread - 1];
+            for (int k = 1; k < kEmitPerLane; ++k) m[k] = max(m[k], m[k - 1]);
+            unsigned int x = m[kEmitPerLane - 1];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
@@ -270,43 +293,66 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
             }
             unsigned int pre = __shfl_up_sync(0xffffffffu, x, 1);
             if (lane == 0) pre = 0u;
-            if (lane == 31) s.warp_tot[warp] = x;
-            __syncthreads();
-            for (int w = 0; w < warp; ++w) pre = max(pre, s.warp_tot[w]);
             o4[0] = make_uint4(max(pre, m[0]), max(pre, m[1]), max(pre, m[2]), max(pre, m[3]));
             o4[1] = make_uint4(max(pre, m[4]), max(pre, m[5]), max(pre, m[6]), max(pre, m[7]));
-            __syncthreads();
-            const unsigned int nwin = block_inst - a < (unsigned int)kEmitWindow ? block_inst - a : kEmitWindow;
-            for (unsigned int jj = tid; jj < nwin; jj += kEmitThreads) {
-                const int lo = (int)s.owner[jj] - 1;
-                const unsigned int j = a + jj;
-                const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
-                const unsigned int rl = s.rect_lo[lo];
-                const unsigned int min_tx = rl & 0xFFFFu, min_ty = rl >> 16;
-                const unsigned int w = s.width[lo];
-                const unsigned int q = j - start;
-                /* q / w through the reciprocal (exact after one correction
-                 * step while q < 2^20), integer division beyond */
-                unsigned int row;
-                if (q < (1u << 20)) {
-                    row = (unsigned int)((float)q * s.rcp_width[lo]);
-                    if (row * w > q) --row;
-                    else if ((row + 1u) * w <= q) ++row;
-                } else {
-                    row = q / w;
+            __syncwarp();
+            const unsigned int nwin = w_end - a < (unsigned int)kEmitWindow ? w_end - a : kEmitWindow;
+            for (unsigned int b0 = 0; b0 < nwin; b0 += 32) {
+                const unsigned int jj = b0 + lane;
+                const bool ok = jj < nwin;
+                unsigned int tile = 0u;
+                bool kept = false;   /* written: within the instance capacity */
+                if (ok) {
+                    const int lo = warp * 32 + (int)own[jj] - 1;
+                    const unsigned int j = a + jj;
+                    const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
+                    const unsigned int rl = s.rect_lo[lo];
+                    const unsigned int min_tx = rl & 0xFFFFu, min_ty = rl >> 16;
+                    const unsigned int w = s.width[lo];
+                    const unsigned int q = j - start;
+                    /* q / w through the reciprocal (exact after one correction
+                     * step while q < 2^20), integer division beyond */
+                    unsigned int row;
+                    if (q < (1u << 20)) {
+                        row = (unsigned int)((float)q * s.rcp_width[lo]);
+                        if (row * w > q) --row;
+                        else if ((row + 1u) * w <= q) ++row;
+                    } else {
+                        row = q / w;
+                    }
+                    const unsigned int col = q - row * w;
+                    /* rows outer, columns inner (pipeline.mojo:152-153) */
+                    tile = s.tile_base[lo] + (min_ty + row) * s.tiles_x[lo] + min_tx + col;
+                    const unsigned long long pos = inst_base + j;
+                    kor |= tile;
+                    knot |= ~tile;
+                    if (pos < (unsigned long long)cap) {
+                        f.keys[0][pos] = tile;
+                        f.vals[0][pos] = s.vis[lo];
+                        kept = true;
+                        atomicAdd(&s.hist[0][tile & 0xFFu], 1u);
+                    }
                 }
-                const unsigned int col = q - row * w;
-                /* rows outer, columns inner (pipeline.mojo:152-153) */
-                const unsigned int tile = s.tile_base[lo] + (min_ty + row) * s.tiles_x[lo] + min_tx + col;
-                const unsigned long long pos = inst_base + j;
-                kor |= tile;
-                knot |= ~tile;
-                if (pos < (unsigned long long)cap) {
-                    f.keys[0][pos] = tile;
-                    f.vals[0][pos] = s.vis[lo];
+                /* only the written instances are counted (the sort takes the
+                 * first `capacity` of them). The higher digits change rarely
+                 * from one instance to the next (a splat's row of tiles):
+                 * each run of equal values over consecutive lanes is counted
+                 * once, by its first lane; the written lanes are a prefix of
+                 * the warp's. */
+                const unsigned int n_kept = __popc(__ballot_sync(0xffffffffu, kept));
+                for (int d = 1; d < nd; ++d) {
+                    const unsigned int dv = kept ? (tile >> (8 * d)) & 0xFFu : 0x100u;
+                    const unsigned int prev = __shfl_up_sync(0xffffffffu, dv, 1);
+                    const bool first = kept && (lane == 0 || prev != dv);
+                    const unsigned int firsts = __ballot_sync(0xffffffffu, first);
+                    if (first) {
+                        const unsigned int later = firsts & ~((2u << lane) - 1u);
+                        const unsigned int run_end = later ? (unsigned int)(__ffs(later) - 1) : n_kept;
+                        atomicAdd(&s.hist[d][dv], run_end - (unsigned int)lane);
+                    }
                 }
             }
-            __syncthreads();
+            __syncwarp();
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -318,6 +364,20 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
             atomicOr(&s.key_or_not, (unsigned long long)knot);
         }
         __syncthreads();
+        for (int d = 0; d < nd; ++d) {
+            const unsigned int c = s.hist[d][tid];
+            if (c) atomicAdd(&ctrl->tile_sort.hist[d][tid], c);
+        }
+        /* look-back descriptors of the sort tiles whose first key is one of
+         * this block's instances (every tile of the sort has one) */
+        {
+            const long long i0 = (long long)inst_base, i1 = (long long)inst_base + block_inst;
+            long long t0 = (i0 + sort_tile_keys - 1) / sort_tile_keys, t1 = (i1 + sort_tile_keys - 1) / sort_tile_keys;
+            if (t1 > sort_lb_tiles) t1 = sort_lb_tiles;
+            for (int d = 0; d < nd; ++d)
+                for (long long j = t0 * 256 + tid; j < t1 * 256; j += kEmitThreads)
+                    sort_lb[(size_t)d * (size_t)sort_lb_tiles * 256 + (size_t)j] = 0u;
+        }
         if (tid == 0) {
             if (block_inst) {
                 atomicOr(&ctrl->tile_sort.key_or, s.key_or);
@@ -639,16 +699,20 @@ void launch_project(const ViewTable* vt, int n_views, const LumenRenderOptions& 
     }
 }
 
+/* sort_lb: the tile sort's look-back region (sort_lb_tiles descriptor
+ * tiles per digit) for digit passes of sort_tile_keys keys per tile. */
 void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, unsigned long long* lb,
-                 long long n_blocks, bool persistent, int num_sms, cudaStream_t st) {
+                 unsigned int* sort_lb, long long sort_lb_tiles, int sort_tile_keys, long long n_blocks,
+                 bool persistent, int num_sms, cudaStream_t st) {
     if (n_blocks <= 0) return;
     if (persistent) {
         const int per_sm = g_emit_per_sm > 0 ? g_emit_per_sm : 1;
-        launch_chained(emit_kernel<true>, dim3(per_sm * num_sms), dim3(kEmitThreads), 0, st, vt, f, ctrl, lb);
+        launch_chained(emit_kernel<true>, dim3(per_sm * num_sms), dim3(kEmitThreads), 0, st, vt, f, ctrl, lb, sort_lb,
+                       sort_lb_tiles, sort_tile_keys);
     } else {
         launch_chained(emit_kernel<false>,
                        dim3((unsigned int)((n_blocks * kProjThreads + kEmitThreads - 1) / kEmitThreads)),
-                       dim3(kEmitThreads), 0, st, vt, f, ctrl, lb);
+                       dim3(kEmitThreads), 0, st, vt, f, ctrl, lb, sort_lb, sort_lb_tiles, sort_tile_keys);
     }
 }
 

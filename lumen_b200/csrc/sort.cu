@@ -192,9 +192,16 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
     constexpr int kTileKeys = kSortThreads * kItems;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PassSmem<KeyT, kItems>& s = *reinterpret_cast<PassSmem<KeyT, kItems>*>(smem_raw);
-    const unsigned int varying = sc->varying;
-    if (!(varying & (1u << digit))) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    /* the digits that vary, from the producer's key statistics (the same
+     * rule as the histogram kernel's, for sorts whose histogram the producer
+     * counted) */
+    const unsigned int varying = sort_count(sc, capacity) > 1 ? varying_digits(sc, (int)sizeof(KeyT)) : 0u;
+    if (blockIdx.x == 0 && tid == 0) {
+        sc->varying = varying;
+        sc->sorted_buffer = (unsigned int)(__popc(varying) & 1);
+    }
+    if (!(varying & (1u << digit))) return;
     const int src = __popc(varying & ((1u << digit) - 1u)) & 1;
     const KeyT* __restrict__ kin = src ? k1 : k0;
     const unsigned int* __restrict__ vin = src ? v1 : v0;
@@ -346,12 +353,15 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
 
 /* binning.mojo:51-73 in parallel, on tile-sorted 32-bit tile ids: a tile's
  * range starts where its id first appears and ends after it last appears.
- * Empty tiles keep the (-1, -1) the histogram kernel wrote.
+ * Empty tiles keep the (-1, -1) written before the sort.
  *
- * Each lane takes 4 consecutive ids per round (one 16-byte load; the
- * frame's key buffers are 16-byte aligned), its neighbours' ids come from
- * the adjacent lanes, and a group of four equal ids between equal
- * neighbours (almost every group) is done after one comparison chain. */
+ * Each lane takes 8 consecutive ids per round (two 16-byte loads; the
+ * frame's key buffers are 16-byte aligned) and its neighbours' ids come
+ * from the adjacent lanes. The ids are sorted, so when the id before the
+ * group equals the id after it, all eight equal it and the group holds no
+ * boundary: one comparison for almost every group. */
+constexpr int kRangeIds = 8;
+
 __global__ void __launch_bounds__(256)
 tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, ViewTable* vt,
                    int* ranges, Control* ctrl) {
@@ -365,26 +375,27 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     unsigned int touched = 0;
     /* the warp's first id, so that the loop and its shuffles are warp-uniform */
-    for (long long wb = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4; wb < K; wb += nthreads * 4) {
-        const long long i0 = wb + 4 * lane;
-        unsigned int k[4];
-        if (i0 + 3 < K) {
-            const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
-            k[0] = q.x; k[1] = q.y; k[2] = q.z; k[3] = q.w;
+    for (long long wb = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * kRangeIds; wb < K;
+         wb += nthreads * kRangeIds) {
+        const long long i0 = wb + kRangeIds * lane;
+        unsigned int k[kRangeIds];
+        if (i0 + kRangeIds - 1 < K) {
+            const uint4 q0 = *reinterpret_cast<const uint4*>(keys + i0);
+            const uint4 q1 = *reinterpret_cast<const uint4*>(keys + i0 + 4);
+            k[0] = q0.x; k[1] = q0.y; k[2] = q0.z; k[3] = q0.w;
+            k[4] = q1.x; k[5] = q1.y; k[6] = q1.z; k[7] = q1.w;
         } else {
 #pragma unroll
-            for (int r = 0; r < 4; ++r) k[r] = i0 + r < K ? keys[i0 + r] : 0xFFFFFFFFu;
+            for (int r = 0; r < kRangeIds; ++r) k[r] = i0 + r < K ? keys[i0 + r] : 0xFFFFFFFFu;
         }
-        const unsigned int up = __shfl_up_sync(0xffffffffu, k[3], 1);
+        const unsigned int up = __shfl_up_sync(0xffffffffu, k[kRangeIds - 1], 1);
         const unsigned int down = __shfl_down_sync(0xffffffffu, k[0], 1);
         if (i0 >= K) continue;
         const unsigned int prev = lane > 0 ? up : (i0 > 0 ? keys[i0 - 1] : 0xFFFFFFFFu);
-        const unsigned int next = lane < 31 ? down : (i0 + 4 < K ? keys[i0 + 4] : 0xFFFFFFFFu);
-        if (i0 > 0 && i0 + 4 < K && prev == k[0] && k[0] == k[1] && k[1] == k[2] && k[2] == k[3] && k[3] == next &&
-            (long long)k[0] < n_tiles)
-            continue;
+        const unsigned int next = lane < 31 ? down : (i0 + kRangeIds < K ? keys[i0 + kRangeIds] : 0xFFFFFFFFu);
+        if (i0 > 0 && i0 + kRangeIds < K && prev == next && (long long)next < n_tiles) continue;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < kRangeIds; ++r) {
             const long long i = i0 + r;
             if (i >= K) break;
             const unsigned int t = k[r];
@@ -393,7 +404,7 @@ tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long cap
                 continue;
             }
             const unsigned int before = r == 0 ? prev : k[r - 1];
-            const unsigned int after = r == 3 ? next : k[r + 1];   /* 0xFFFFFFFF past the end */
+            const unsigned int after = r == kRangeIds - 1 ? next : k[r + 1];   /* 0xFFFFFFFF past the end */
             if (i == 0 || before != t) {
                 ranges[2 * (size_t)t] = (int)i;
                 ++touched;
@@ -455,9 +466,10 @@ __global__ void sorted_keys64_kernel(const unsigned int* k0, const unsigned int*
 template <typename KeyT, int kItems>
 void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                       unsigned int* lb, long long lb_tiles_cap, int* ranges, const long long* n_range_tiles,
-                      unsigned int* err, int key_bytes, int num_sms, cudaStream_t st) {
-    launch_chained(histogram_kernel<KeyT>, dim3(num_sms * 4), dim3(256), 0, st, (const KeyT*)k0, capacity, sc, lb,
-                   lb_tiles_cap, kSortThreads * kItems, ranges, n_range_tiles);
+                      unsigned int* err, int key_bytes, int num_sms, cudaStream_t st, bool counted = false) {
+    if (!counted)
+        launch_chained(histogram_kernel<KeyT>, dim3(num_sms * 4), dim3(256), 0, st, (const KeyT*)k0, capacity, sc, lb,
+                       lb_tiles_cap, kSortThreads * kItems, ranges, n_range_tiles);
     const size_t smem = sizeof(PassSmem<KeyT, kItems>);
     /* matches __launch_bounds__: all CTAs resident */
     const int ctas_per_sm = sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : kItems <= 16 ? 3 : 2) : 2;
@@ -485,6 +497,23 @@ void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigne
                                            err, key_bytes, num_sms, st);
 }
 
+/* The frame's tile sort when the emission has counted the digit values,
+ * cleared the look-back tiles and filled the ranges: the digit passes
+ * only. */
+void launch_tile_sort_counted(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1,
+                              long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap,
+                              unsigned int* err, int items, int key_bytes, int num_sms, cudaStream_t st) {
+    if (items == 8)
+        launch_sort_impl<unsigned int, 8>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
+                                          key_bytes, num_sms, st, true);
+    else if (items == 24)
+        launch_sort_impl<unsigned int, 24>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
+                                           key_bytes, num_sms, st, true);
+    else
+        launch_sort_impl<unsigned int, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
+                                           key_bytes, num_sms, st, true);
+}
+
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
                    long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap, unsigned int* err,
                    int num_sms, cudaStream_t st) {
@@ -493,9 +522,9 @@ void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long*
 }
 
 void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st) {
-    /* about one group of 4 keys per thread at full capacity (the loads are
+    /* about one group of 8 ids per thread at full capacity (the loads are
      * independent, so more threads in flight hide their latency) */
-    long long grid = ((long long)f.instance_capacity + 1023) / 1024;
+    long long grid = ((long long)f.instance_capacity + 256 * kRangeIds - 1) / (256 * kRangeIds);
     if (grid < num_sms * 4) grid = num_sms * 4;
     if (grid > (1ll << 20)) grid = 1ll << 20;
     launch_chained(tile_ranges_kernel, dim3((unsigned int)grid), dim3(256), 0, st, (const unsigned int*)f.keys[0],
