@@ -211,7 +211,7 @@ LumenStatus lumen_gpu_stage_timer_read(LumenGpuStageTimer* timer, float stage_ms
  * composite_chunk: sorted instances the compositor stages per round (128,
  * 256 or 512); *_sort_items: keys per thread in a digit pass of the depth
  * and tile sorts (depth: 8 or 16; tile: 8, 16 or 24 — tiles of 2048, 4096
- * or 6144 keys). Defaults 512, 8, 16. */
+ * or 6144 keys). Defaults 512, 16, 16. */
 typedef struct {
     int32_t composite_chunk;
     int32_t depth_sort_items;

@@ -178,20 +178,101 @@ constexpr int kEmitPerLane = kEmitWindow / 32;
 static_assert(kEmitPerLane == 8, "two 16-byte slot groups per lane");
 
 struct EmitSmem {
-    __align__(16) unsigned int owner[kEmitThreads / 32][kEmitWindow];   /* 1 + the warp lane of each window slot */
+    /* per warp and window slot: 1 + the lane whose splat holds the instance */
+    __align__(16) unsigned int owner[kEmitThreads / 32][kEmitWindow];
     unsigned int blk;
     unsigned int warp_tot[kEmitThreads / 32];
     unsigned long long inst_base;
-    unsigned int incl[kEmitThreads];
-    unsigned int vis[kEmitThreads];
-    unsigned int rect_lo[kEmitThreads];   /* min_tx | min_ty << 16 */
-    unsigned int width[kEmitThreads];     /* tiles per rectangle row */
-    unsigned int tile_base[kEmitThreads]; /* batch-wide id of the view's tile 0 */
-    unsigned int tiles_x[kEmitThreads];
-    float rcp_width[kEmitThreads];        /* 1 / width, for the row of an instance */
+    /* per splat: its first instance (block-relative), tiles per rectangle
+     * row, the batch-wide id of its first tile, tiles per view row */
+    uint4 run[kEmitThreads];
+    /* per splat: 1 / (tiles per rectangle row), as bits, for the row of an
+     * instance; its visible index */
+    uint2 aux[kEmitThreads];
     unsigned int hist[3][256];            /* the block's tile ids: counts of each digit value */
     unsigned long long key_or, key_or_not;
 };
+
+/* Owners of the warp's window [a, a + kEmitWindow): slot k of s.owner[warp]
+ * gets 1 + the lane whose splat holds instance a + k (block-relative). Returns
+ * the window's instance count. */
+__device__ __forceinline__ unsigned int emit_window_owners(EmitSmem& s, int warp, int lane, unsigned int a,
+                                                           unsigned int excl, unsigned int cnt, unsigned int w_end) {
+    unsigned int* own = s.owner[warp];
+    uint4* o4 = reinterpret_cast<uint4*>(own) + lane * 2;
+    o4[0] = make_uint4(0u, 0u, 0u, 0u);
+    o4[1] = make_uint4(0u, 0u, 0u, 0u);
+    __syncwarp();
+    if (cnt && excl + cnt > a && excl < a + kEmitWindow) own[(excl > a ? excl : a) - a] = (unsigned int)lane + 1u;
+    __syncwarp();
+    /* inclusive prefix maximum: eight consecutive slots per lane, then
+     * across the lanes */
+    const uint4 g0 = o4[0], g1 = o4[1];
+    unsigned int m[kEmitPerLane] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+    for (int k = 1; k < kEmitPerLane; ++k) m[k] = max(m[k], m[k - 1]);
+    unsigned int x = m[kEmitPerLane - 1];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    unsigned int pre = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) pre = 0u;
+    o4[0] = make_uint4(max(pre, m[0]), max(pre, m[1]), max(pre, m[2]), max(pre, m[3]));
+    o4[1] = make_uint4(max(pre, m[4]), max(pre, m[5]), max(pre, m[6]), max(pre, m[7]));
+    __syncwarp();
+    return w_end - a < (unsigned int)kEmitWindow ? w_end - a : kEmitWindow;
+}
+
+/* Batch-wide tile id of block-relative instance j of splat lo: rows outer,
+ * columns inner (pipeline.mojo:152-153). */
+__device__ __forceinline__ unsigned int emit_tile(const EmitSmem& s, int lo, unsigned int j) {
+    const uint4 rn = s.run[lo];
+    const unsigned int w = rn.y;
+    const unsigned int q = j - rn.x;
+    /* q / w through the reciprocal (exact after one correction step while
+     * q < 2^20), integer division beyond */
+    unsigned int row;
+    if (q < (1u << 20)) {
+        row = (unsigned int)((float)q * __uint_as_float(s.aux[lo].x));
+        if (row * w > q) --row;
+        else if ((row + 1u) * w <= q) ++row;
+    } else {
+        row = q / w;
+    }
+    return rn.z + row * rn.w + (q - row * w);
+}
+
+/* Writes the instance at pos when it is within the capacity; counts its low
+ * tile-id digit. Returns whether it was written. */
+__device__ __forceinline__ bool emit_store(const LumenGpuFrame& f, EmitSmem& s, unsigned long long pos,
+                                           long long cap, unsigned int tile, int lo) {
+    if (pos >= (unsigned long long)cap) return false;
+    f.keys[0][pos] = tile;
+    f.vals[0][pos] = s.aux[lo].y;
+    atomicAdd(&s.hist[0][tile & 0xFFu], 1u);
+    return true;
+}
+
+/* The higher tile-id digits of the warp's written instances (a prefix of
+ * its lanes). They change rarely from one instance to the next (a splat's
+ * row of tiles): each run of equal values over consecutive lanes is counted
+ * once, by its first lane. */
+__device__ __forceinline__ void emit_count(EmitSmem& s, int lane, int nd, unsigned int tile, bool kept) {
+    const unsigned int n_kept = __popc(__ballot_sync(0xffffffffu, kept));
+    for (int d = 1; d < nd; ++d) {
+        const unsigned int dv = kept ? (tile >> (8 * d)) & 0xFFu : 0x100u;
+        const unsigned int prev = __shfl_up_sync(0xffffffffu, dv, 1);
+        const bool first = kept && (lane == 0 || prev != dv);
+        const unsigned int firsts = __ballot_sync(0xffffffffu, first);
+        if (first) {
+            const unsigned int later = firsts & ~((2u << lane) - 1u);
+            const unsigned int run_end = later ? (unsigned int)(__ffs(later) - 1) : n_kept;
+            atomicAdd(&s.hist[d][dv], run_end - (unsigned int)lane);
+        }
+    }
+}
 
 /* Like project_kernel: 256 consecutive splats of the depth order per ticket.
  * Tile ids are batch-wide (view tile_begin + ty * tiles_x + tx).
@@ -203,7 +284,7 @@ struct EmitSmem {
  * 256 * sort_items-key tiles that start among its instances, and fills the
  * tile ranges with (-1, -1). */
 template <bool kPersistent>
-__global__ void __launch_bounds__(kEmitThreads)
+__global__ void __launch_bounds__(kEmitThreads, 8)
 emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, unsigned long long* lb,
             unsigned int* sort_lb, long long sort_lb_tiles, int sort_tile_keys) {
     chain_begin();
@@ -231,26 +312,23 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         const int blk = (int)s.blk;
         if ((long long)blk * kEmitThreads >= V) break;   /* past the visible splats: no look-back waits on it */
         const long long p = (long long)blk * kEmitThreads + tid;
-        unsigned int cnt = 0, v = 0;
+        unsigned int cnt = 0, v = 0, w = 1, tile0 = 0, tiles_x = 0;
         if (p < V) {
             v = order[p];
             const unsigned long long r = f.rects[v];
             const int mnx = rect_min_tx(r), mny = rect_min_ty(r);
-            const unsigned int w = (unsigned int)(rect_max_tx(r) - mnx + 1);
+            w = (unsigned int)(rect_max_tx(r) - mnx + 1);
             const unsigned int h = (unsigned int)(rect_max_ty(r) - mny + 1);
             cnt = w * h;
             const ViewDesc& vd = vt->view[rect_view(r)];
-            s.rect_lo[tid] = (unsigned int)mnx | ((unsigned int)mny << 16);
-            s.width[tid] = w;
-            s.tile_base[tid] = (unsigned int)vd.tile_begin;
-            s.tiles_x[tid] = (unsigned int)vd.tiles_x;
-            s.rcp_width[tid] = 1.0f / (float)w;
+            tiles_x = (unsigned int)vd.tiles_x;
+            tile0 = (unsigned int)vd.tile_begin + (unsigned int)mny * tiles_x + (unsigned int)mnx;
         }
         unsigned int block_inst = 0;
         const unsigned int excl = block_exclusive_scan<kEmitThreads>(cnt, s.warp_tot, &block_inst);
         if (tid == 0) st_volatile_u64(lb + blk, (blk == 0 ? kDescIncl64 : kDescAgg64) | block_inst);
-        s.incl[tid] = excl + cnt;
-        s.vis[tid] = v;
+        s.run[tid] = make_uint4(excl, w, tile0, tiles_x);
+        s.aux[tid] = make_uint2(__float_as_uint(1.0f / (float)w), v);
         if (warp == 0) {
             const unsigned long long e = blk > 0 ? lookback64(lb, blk, &ctrl->error_flags) : 0ull;
             if (lane == 0) {
@@ -271,86 +349,20 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         const unsigned int my_end = excl + cnt;
         const unsigned int w_begin = __shfl_sync(0xffffffffu, excl, 0);
         const unsigned int w_end = __shfl_sync(0xffffffffu, my_end, 31);
-        unsigned int* own = s.owner[warp];
-        uint4* o4 = reinterpret_cast<uint4*>(own) + lane * 2;
         for (unsigned int a = w_begin; a < w_end; a += kEmitWindow) {
-            o4[0] = make_uint4(0u, 0u, 0u, 0u);
-            o4[1] = make_uint4(0u, 0u, 0u, 0u);
-            __syncwarp();
-            if (cnt && my_end > a && excl < a + kEmitWindow) own[(excl > a ? excl : a) - a] = (unsigned int)lane + 1u;
-            __syncwarp();
-            /* inclusive prefix maximum: eight consecutive slots per lane,
-             * then across the lanes */
-            const uint4 g0 = o4[0], g1 = o4[1];
-            unsigned int m[kEmitPerLane] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
-#pragma unroll
-            for (int k = 1; k < kEmitPerLane; ++k) m[k] = max(m[k], m[k - 1]);
-            unsigned int x = m[kEmitPerLane - 1];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x = max(x, y);
-            }
-            unsigned int pre = __shfl_up_sync(0xffffffffu, x, 1);
-            if (lane == 0) pre = 0u;
-            o4[0] = make_uint4(max(pre, m[0]), max(pre, m[1]), max(pre, m[2]), max(pre, m[3]));
-            o4[1] = make_uint4(max(pre, m[4]), max(pre, m[5]), max(pre, m[6]), max(pre, m[7]));
-            __syncwarp();
-            const unsigned int nwin = w_end - a < (unsigned int)kEmitWindow ? w_end - a : kEmitWindow;
+            const unsigned int nwin = emit_window_owners(s, warp, lane, a, excl, cnt, w_end);
             for (unsigned int b0 = 0; b0 < nwin; b0 += 32) {
                 const unsigned int jj = b0 + lane;
-                const bool ok = jj < nwin;
                 unsigned int tile = 0u;
-                bool kept = false;   /* written: within the instance capacity */
-                if (ok) {
-                    const int lo = warp * 32 + (int)own[jj] - 1;
-                    const unsigned int j = a + jj;
-                    const unsigned int start = lo > 0 ? s.incl[lo - 1] : 0u;
-                    const unsigned int rl = s.rect_lo[lo];
-                    const unsigned int min_tx = rl & 0xFFFFu, min_ty = rl >> 16;
-                    const unsigned int w = s.width[lo];
-                    const unsigned int q = j - start;
-                    /* q / w through the reciprocal (exact after one correction
-                     * step while q < 2^20), integer division beyond */
-                    unsigned int row;
-                    if (q < (1u << 20)) {
-                        row = (unsigned int)((float)q * s.rcp_width[lo]);
-                        if (row * w > q) --row;
-                        else if ((row + 1u) * w <= q) ++row;
-                    } else {
-                        row = q / w;
-                    }
-                    const unsigned int col = q - row * w;
-                    /* rows outer, columns inner (pipeline.mojo:152-153) */
-                    tile = s.tile_base[lo] + (min_ty + row) * s.tiles_x[lo] + min_tx + col;
-                    const unsigned long long pos = inst_base + j;
+                bool kept = false;
+                if (jj < nwin) {
+                    const int lo = warp * 32 + (int)s.owner[warp][jj] - 1;
+                    tile = emit_tile(s, lo, a + jj);
                     kor |= tile;
                     knot |= ~tile;
-                    if (pos < (unsigned long long)cap) {
-                        f.keys[0][pos] = tile;
-                        f.vals[0][pos] = s.vis[lo];
-                        kept = true;
-                        atomicAdd(&s.hist[0][tile & 0xFFu], 1u);
-                    }
+                    kept = emit_store(f, s, inst_base + a + jj, cap, tile, lo);
                 }
-                /* only the written instances are counted (the sort takes the
-                 * first `capacity` of them). The higher digits change rarely
-                 * from one instance to the next (a splat's row of tiles):
-                 * each run of equal values over consecutive lanes is counted
-                 * once, by its first lane; the written lanes are a prefix of
-                 * the warp's. */
-                const unsigned int n_kept = __popc(__ballot_sync(0xffffffffu, kept));
-                for (int d = 1; d < nd; ++d) {
-                    const unsigned int dv = kept ? (tile >> (8 * d)) & 0xFFu : 0x100u;
-                    const unsigned int prev = __shfl_up_sync(0xffffffffu, dv, 1);
-                    const bool first = kept && (lane == 0 || prev != dv);
-                    const unsigned int firsts = __ballot_sync(0xffffffffu, first);
-                    if (first) {
-                        const unsigned int later = firsts & ~((2u << lane) - 1u);
-                        const unsigned int run_end = later ? (unsigned int)(__ffs(later) - 1) : n_kept;
-                        atomicAdd(&s.hist[d][dv], run_end - (unsigned int)lane);
-                    }
-                }
+                emit_count(s, lane, nd, tile, kept);
             }
             __syncwarp();
         }
@@ -371,12 +383,18 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
         /* look-back descriptors of the sort tiles whose first key is one of
          * this block's instances (every tile of the sort has one) */
         {
-            const long long i0 = (long long)inst_base, i1 = (long long)inst_base + block_inst;
-            long long t0 = (i0 + sort_tile_keys - 1) / sort_tile_keys, t1 = (i1 + sort_tile_keys - 1) / sort_tile_keys;
-            if (t1 > sort_lb_tiles) t1 = sort_lb_tiles;
-            for (int d = 0; d < nd; ++d)
-                for (long long j = t0 * 256 + tid; j < t1 * 256; j += kEmitThreads)
-                    sort_lb[(size_t)d * (size_t)sort_lb_tiles * 256 + (size_t)j] = 0u;
+            /* only the first `capacity` instances are sorted (capacity < 2^30) */
+            const unsigned long long ucap = (unsigned long long)cap;
+            const unsigned long long e0 = inst_base, e1 = inst_base + block_inst;
+            const unsigned int i0 = (unsigned int)(e0 < ucap ? e0 : ucap), i1 = (unsigned int)(e1 < ucap ? e1 : ucap);
+            const unsigned int tk = (unsigned int)sort_tile_keys;
+            const unsigned int t0 = (i0 + tk - 1u) / tk;
+            unsigned int t1 = (i1 + tk - 1u) / tk;
+            if ((long long)t1 > sort_lb_tiles) t1 = (unsigned int)sort_lb_tiles;
+            for (int d = 0; d < nd; ++d) {
+                unsigned int* region = sort_lb + (size_t)d * (size_t)sort_lb_tiles * 256;
+                for (unsigned int j = t0 * 256u + (unsigned int)tid; j < t1 * 256u; j += kEmitThreads) region[j] = 0u;
+            }
         }
         if (tid == 0) {
             if (block_inst) {

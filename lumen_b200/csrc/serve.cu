@@ -47,8 +47,8 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
 namespace {
 
 constexpr int kVariants = 6;
-const LaunchConfig kVariantTable[kVariants] = {{256, 8, 16}, {128, 8, 16}, {512, 8, 16},
-                                                {256, 8, 8},  {128, 8, 8},  {512, 8, 8}};
+const LaunchConfig kVariantTable[kVariants] = {{256, 16, 16}, {128, 16, 16}, {512, 16, 16},
+                                                {256, 16, 8},  {128, 16, 8},  {512, 16, 8}};
 
 int variant_of(int chunk, int items) {
     for (int i = 0; i < kVariants; ++i)

@@ -70,15 +70,15 @@ constexpr int kSort64Tile = kSortThreads * kSort64Items;
 struct LaunchConfig {
     int composite_chunk;   /* instances staged per compositing round: 128, 256 or 512 */
     int depth_sort_items;  /* keys per thread in a depth-sort digit pass: 8 or 16 */
-    int tile_sort_items;   /* keys per thread in a tile-sort digit pass: 8 or 16 */
+    int tile_sort_items;   /* keys per thread in a tile-sort digit pass: 8, 16 or 24 */
     int track;             /* 1: some view's image asks for contributor counts or last-visited
                               offsets (the compositor then keeps them); set by the host */
 };
 /* measured on B200 at 1080p with 1 M Gaussians: 512-instance compositor
- * chunks (0.233 against 0.238 ms for 256, 0.259 for 128); 2048-key tiles
- * shorten the (smaller) depth sort, 4096-key tiles suit the tile sort
- * (0.234 ms against 0.256 for 2048 and 0.243 for 6144) */
-constexpr LaunchConfig kDefaultLaunch = {512, 8, 16, 1};
+ * chunks (0.233 against 0.238 ms for 256, 0.259 for 128); 4096-key tiles
+ * for both sorts (sort stage 0.1955 ms, against 0.1978 with 2048-key depth
+ * tiles, 0.2002 with 6144-key and 0.2232 with 2048-key tile-sort tiles) */
+constexpr LaunchConfig kDefaultLaunch = {512, 16, 16, 1};
 
 __host__ __device__ constexpr inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
