@@ -45,12 +45,16 @@ struct LumenCloud {
     unsigned long long generation;   /* changes on every mutation */
 };
 
+/* Row bands per lumen_rasterize frame (the read-back of a band overlaps
+ * the compositing of the next). */
+constexpr int kRasterBands = 4;
+
 struct LumenRasterizer {
     LumenConfig config;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;   /* frame-buffer copies, overlapping the render */
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_up = nullptr, ev_down = nullptr;
-    cudaEvent_t ev_band[4] = {};          /* one per compositor band (kRasterBands) */
+    cudaEvent_t ev_band[kRasterBands] = {};   /* one per compositor band */
     LumenGpuRenderer* renderer = nullptr;
     /* device mirror of the last cloud rendered */
     const LumenCloud* cached_cloud = nullptr;
@@ -216,7 +220,6 @@ bool create_band_events(LumenRasterizer* r) {
  * the copy stream reads them back while the next band is composited (the
  * copy engines need no SM, so the read-back is not held up by the
  * compositor's blocks). */
-constexpr int kRasterBands = 4;
 
 struct BandCopy {
     LumenRasterizer* r;
