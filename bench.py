@@ -41,17 +41,19 @@ N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
 # DRAM bytes (read + write) of one composite_kernel<512> launch at the 1 M-Gaussian
 # 1080p workload, from an ncu capture (profiles/forward_config1_kernels.md)
-COMPOSITE_DRAM_BYTES = 42.6e6
+COMPOSITE_DRAM_BYTES = 43.1e6
 def kernels_per_frame(n_tiles: int) -> int:
-    """Kernels one forward frame launches: init, project, the depth sort's
-    histogram and 4 digit passes, emit, the tile sort's histogram and one
-    digit pass per byte a tile id can vary in, tile ranges, composite."""
+    """Kernels one forward frame launches: init; the projection's count,
+    offset scan and projection; the depth sort's histogram and 4 digit
+    passes; the emission (which also counts the tile sort's digits); one
+    tile-sort digit pass per byte a tile id can vary in; tile ranges;
+    composite."""
     tile_bytes = 0
     t = n_tiles - 1
     while t > 0:
         tile_bytes += 1
         t >>= 8
-    return 1 + 1 + (1 + 4) + 1 + (1 + tile_bytes) + 1 + 1
+    return 1 + 3 + (1 + 4) + 1 + tile_bytes + 1 + 1
 
 
 def parse():
