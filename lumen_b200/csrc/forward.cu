@@ -10,9 +10,10 @@
  *   batch_project      K1c: projection, cull, SH, records and depth keys at those offsets
  *   histogram<u32>     depth-key digits of the visible splats
  *   onesweep_pass x4   stable sort of visible splats by depth key
- *   emit               K2: (tile id, visible index) per covered tile, in depth order
- *   histogram<u32>     tile-id digits; ranges = -1
- *   onesweep_pass x4   stable sort of instances by tile id
+ *   emit               K2: (tile id, visible index) per covered tile, in depth order;
+ *                      also the tile sort's digit counts, look-back tiles and ranges = -1
+ *   onesweep_pass xb   stable sort of instances by tile id (b: the bytes a tile id
+ *                      can vary in; with no Gaussians a histogram launch comes first)
  *   tile_ranges        K4
  *   composite          K5
  * Passes whose digit is constant exit at once (decided on the device).

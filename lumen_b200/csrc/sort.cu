@@ -8,10 +8,12 @@
  *
  * B200 design (onesweep, Adinets & Merrill 2022), for 32- or 64-bit keys:
  *  - one histogram pass reads the keys once and counts every digit that
- *    varies. A digit is constant when no two keys differ in that byte (the
- *    OR of all keys and the OR of all complemented keys, gathered by the
- *    kernel that produced them, tell which); a pass over a constant digit
- *    leaves a stable sort unchanged, so it is skipped on the device.
+ *    varies (the frame's tile sort needs none: the emission that writes the
+ *    tile ids counts them). A digit is constant when no two keys differ in
+ *    that byte (the OR of all keys and the OR of all complemented keys,
+ *    gathered by the kernel that produced them, tell which); a pass over a
+ *    constant digit leaves a stable sort unchanged, so it is skipped on the
+ *    device.
  *  - each digit pass is one persistent kernel: a CTA takes 4096-key tiles in
  *    ticket order, counts the tile's digits and publishes the counts at
  *    once, ranks its keys with a warp-level multisplit (a shared match mask
