@@ -189,9 +189,10 @@ struct EmitSmem {
     /* per splat: 1 / (tiles per rectangle row), as bits, for the row of an
      * instance; its visible index */
     uint2 aux[kEmitThreads];
-    unsigned int hist[3][256];            /* the block's tile ids: counts of each digit value */
+    unsigned int hist[4][256];            /* the block's tile ids: counts of each digit value */
     unsigned long long key_or, key_or_not;
 };
+static_assert(kEmitThreads == 256, "one emission thread per digit value clears and adds the block's counts");
 
 /* Owners of the warp's window [a, a + kEmitWindow): slot k of s.owner[warp]
  * gets 1 + the lane whose splat holds instance a + k (block-relative). Returns
@@ -296,7 +297,7 @@ emit_kernel(const ViewTable* __restrict__ vt, LumenGpuFrame f, Control* ctrl, un
     /* the tile-id bytes that can vary: ids are below the batch's tile count */
     const long long n_tiles = vt->hdr.total_tiles;
     int nd = 0;
-    for (long long t = n_tiles - 1; t > 0 && nd < 3; t >>= 8) ++nd;
+    for (long long t = n_tiles - 1; t > 0 && nd < 4; t >>= 8) ++nd;
     {
         const long long nthreads = (long long)gridDim.x * blockDim.x;
         for (long long j = (long long)blockIdx.x * blockDim.x + tid; j < 2 * n_tiles; j += nthreads) f.ranges[j] = -1;
