@@ -13,23 +13,26 @@ __device__ __forceinline__ int warp_block_x(int w) { return (w & 1) * 8; }
 __device__ __forceinline__ int warp_block_y(int w) { return (w >> 1) * 4; }
 
 /* Minimum of q(x, y) = a x^2 + 2 b x y + c y^2 over [x0,x1] x [y0,y1]
- * (a > 0, c > 0, ac > b^2): 0 if the origin is inside, otherwise the least
- * of the four edge minima (q is convex along each edge). */
+ * (a > 0, c > 0, ac > b^2): 0 if the origin (q's minimum) is inside,
+ * otherwise the least of the minima over the edges that face the origin:
+ * the segment from the origin to any point p of the rectangle enters it
+ * through such an edge, at a point t p (0 < t <= 1) where q = t^2 q(p) <=
+ * q(p). At most one vertical and one horizontal edge face the origin (the
+ * edge x = x0 when x0 > 0, x = x1 when x1 < 0, and likewise in y); q is
+ * convex along each edge, so its minimum there is at the clamped
+ * stationary point. Branch-free: both edges are evaluated and the ones that
+ * do not face the origin are dropped. */
 __device__ __forceinline__ float quad_min_rect(float a, float b, float c, float b_over_a, float b_over_c,
                                                float x0, float x1, float y0, float y1) {
-    if (x0 <= 0.0f && x1 >= 0.0f && y0 <= 0.0f && y1 >= 0.0f) return 0.0f;
-    float m = INFINITY;
-    const float xs[2] = {x0, x1}, ys[2] = {y0, y1};
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const float x = xs[k];
-        const float y = fminf(fmaxf(-b_over_c * x, y0), y1);
-        m = fminf(m, a * x * x + 2.0f * b * x * y + c * y * y);
-        const float yy = ys[k];
-        const float xx = fminf(fmaxf(-b_over_a * yy, x0), x1);
-        m = fminf(m, a * xx * xx + 2.0f * b * xx * yy + c * yy * yy);
-    }
-    return m;
+    const float x = x0 > 0.0f ? x0 : x1;   /* the vertical edge nearer the origin */
+    const float y = y0 > 0.0f ? y0 : y1;
+    const float ye = fminf(fmaxf(-b_over_c * x, y0), y1);
+    const float xe = fminf(fmaxf(-b_over_a * y, x0), x1);
+    const float mv = a * x * x + 2.0f * b * x * ye + c * ye * ye;
+    const float mh = a * xe * xe + 2.0f * b * xe * y + c * y * y;
+    const bool fv = x0 > 0.0f || x1 < 0.0f, fh = y0 > 0.0f || y1 < 0.0f;
+    if (!fv && !fh) return 0.0f;   /* the origin is inside */
+    return fminf(fv ? mv : INFINITY, fh ? mh : INFINITY);
 }
 
 /* The power above which a splat cannot be blended at any pixel: the
