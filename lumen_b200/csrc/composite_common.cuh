@@ -50,9 +50,16 @@ __device__ __forceinline__ float splat_power_cutoff(float opacity) {
  * centre of warp w's block. A pixel is blended only if
  * power <= 4.5 and opacity * exp(-power) >= 1/255 (compositor.mojo:62-89,
  * :33-35), i.e. 2 * power <= 2 * min(4.5, ln(255 * opacity)); the test uses
- * that bound with a 0.1% + 0.01 margin, far above the float rounding of
- * power, so culling never removes a splat that the per-pixel loop would
- * blend and the results are unchanged. */
+ * that bound with a 0.1% + 0.01 margin, plus a margin for the rounding of
+ * the two float evaluations (the block's minimum here, a pixel's power in
+ * the blend): each is within a few units in the last place of the sum of
+ * the absolute terms, |a| x^2 + 2 |b x y| + |c| y^2 <= S (x^2 + y^2) with
+ * S = |a| + |c| + 2 |b|, so 1e-6 S R^2 (R^2 bounding x^2 + y^2 over the
+ * tile's pixel centres, about 16 float ulps) covers both. That term matters only for
+ * needle-like splats (conic condition numbers above about 1e4, whose terms
+ * cancel); for the others the fixed margin dominates. Culling therefore
+ * never removes a splat that the per-pixel loop would blend and the
+ * results are unchanged. */
 __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float tile_x0, float tile_y0) {
     const float a = con.x, b = con.y, c = con.z, op = geo.w;
     if (!(a > 0.0f && c > 0.0f && a * c - b * b > 0.0f) || !isfinite(a * c)) return 0xFFu;
@@ -60,12 +67,17 @@ __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float
     if (pcut < 0.0f) return 0u;
     const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
     const float b_over_a = b * __frcp_rn(a), b_over_c = b * __frcp_rn(c);
+    /* R^2 over the whole tile's pixel centres bounds it for every block */
+    const float tx0 = tile_x0 + 0.5f - geo.x, tx1 = tx0 + (float)(kTile - 1);
+    const float ty0 = tile_y0 + 0.5f - geo.y, ty1 = ty0 + (float)(kTile - 1);
+    const float r2 = fmaxf(tx0 * tx0, tx1 * tx1) + fmaxf(ty0 * ty0, ty1 * ty1);
+    const float thr = qcut + 1e-6f * (fabsf(a) + fabsf(c) + 2.0f * fabsf(b)) * r2;
     unsigned int m = 0;
 #pragma unroll
     for (int w = 0; w < kTilePixels / 32; ++w) {
         const float x0 = tile_x0 + (float)warp_block_x(w) + 0.5f - geo.x;
         const float y0 = tile_y0 + (float)warp_block_y(w) + 0.5f - geo.y;
-        if (quad_min_rect(a, b, c, b_over_a, b_over_c, x0, x0 + 7.0f, y0, y0 + 3.0f) <= qcut) m |= 1u << w;
+        if (quad_min_rect(a, b, c, b_over_a, b_over_c, x0, x0 + 7.0f, y0, y0 + 3.0f) <= thr) m |= 1u << w;
     }
     return m;
 }
