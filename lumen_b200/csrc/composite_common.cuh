@@ -28,8 +28,11 @@ __device__ __forceinline__ float quad_min_rect(float a, float b, float c, float 
     const float y = y0 > 0.0f ? y0 : y1;
     const float ye = fminf(fmaxf(-b_over_c * x, y0), y1);
     const float xe = fminf(fmaxf(-b_over_a * y, x0), x1);
-    const float mv = a * x * x + 2.0f * b * x * ye + c * ye * ye;
-    const float mh = a * xe * xe + 2.0f * b * xe * y + c * y * y;
+    /* fused multiply-adds (this is a conservative filter, not the blend's
+     * arithmetic; its rounding is covered by the caller's margin) */
+    const float b2 = 2.0f * b;
+    const float mv = __fmaf_rn(c * ye, ye, __fmaf_rn(b2 * x, ye, a * x * x));
+    const float mh = __fmaf_rn(a * xe, xe, __fmaf_rn(b2 * xe, y, c * y * y));
     const bool fv = x0 > 0.0f || x1 < 0.0f, fh = y0 > 0.0f || y1 < 0.0f;
     if (!fv && !fh) return 0.0f;   /* the origin is inside */
     return fminf(fv ? mv : INFINITY, fh ? mh : INFINITY);
@@ -66,7 +69,12 @@ __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float
     const float pcut = fminf(4.5f, __logf(op / min_alpha()) + 0.01f);
     if (pcut < 0.0f) return 0u;
     const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
-    const float b_over_a = b * __frcp_rn(a), b_over_c = b * __frcp_rn(c);
+    /* the stationary points only need to be close: an error d in one moves
+     * the edge's value by c d^2 (second order) */
+    float ra, rc;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(a));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(c));
+    const float b_over_a = b * ra, b_over_c = b * rc;
     /* R^2 over the whole tile's pixel centres bounds it for every block */
     const float tx0 = tile_x0 + 0.5f - geo.x, tx1 = tx0 + (float)(kTile - 1);
     const float ty0 = tile_y0 + 0.5f - geo.y, ty1 = ty0 + (float)(kTile - 1);
