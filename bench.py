@@ -41,7 +41,7 @@ N_GAUSSIANS = 1_000_000
 WIDTH, HEIGHT = 1920, 1080
 # DRAM bytes (read + write) of one composite_kernel<512> launch at the 1 M-Gaussian
 # 1080p workload, from an ncu capture (profiles/forward_config1_kernels.md)
-COMPOSITE_DRAM_BYTES = 44.2e6
+COMPOSITE_DRAM_BYTES = 43.5e6
 def kernels_per_frame(n_tiles: int) -> int:
     """Kernels one forward frame launches: init; the projection's count,
     offset scan and projection; the depth sort's histogram and 4 digit
