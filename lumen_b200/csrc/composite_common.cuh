@@ -4,6 +4,8 @@
  */
 #pragma once
 
+#include <cfloat>
+
 #include "splat_common.cuh"
 
 namespace lumen {
@@ -65,7 +67,9 @@ __device__ __forceinline__ float splat_power_cutoff(float opacity) {
  * results are unchanged. */
 __device__ __forceinline__ unsigned int reach_mask(float4 geo, float4 con, float tile_x0, float tile_y0) {
     const float a = con.x, b = con.y, c = con.z, op = geo.w;
-    if (!(a > 0.0f && c > 0.0f && a * c - b * b > 0.0f) || !isfinite(a * c)) return 0xFFu;
+    /* degenerate, non-finite or subnormal conics (whose approximate
+     * reciprocals below flush to infinity): every block, as the blend decides */
+    if (!(a >= FLT_MIN && c >= FLT_MIN && a * c - b * b > 0.0f) || !isfinite(a * c)) return 0xFFu;
     const float pcut = fminf(4.5f, __logf(op / min_alpha()) + 0.01f);
     if (pcut < 0.0f) return 0u;
     const float qcut = 2.0f * pcut * 1.001f + 1e-3f;
