@@ -940,26 +940,41 @@ def ncu_counters():
     return rows
 
 
-def kernels_table(line, hbm_peak):
+SMS, SCHEDULERS_PER_SM = 148, 4
+
+
+def kernels_table(line, hbm_peak, sm_mhz=1965.0):
     """Each stage of the forward (configuration 1) and of the backward
     (configuration 3): live CUDA-event milliseconds, algorithmic bytes and
     their fraction of the HBM peak, and the instruction-issue and pipe
     figures of its kernels from the latest ncu capture. A stage whose
-    kernels are issue-bound reports that as its bound."""
+    kernels are issue-bound reports that as its bound.
+
+    issue_roofline is the compute-side bound of a stage: its kernels' warp
+    instructions (ncu's count, summed over the stage's launches) over the
+    GPU's issue rate, one warp instruction per scheduler per cycle (148 SMs
+    x 4 schedulers x sm_mhz), against the live stage time."""
     counters = ncu_counters()
     rows = []
+    issue_rate = SMS * SCHEDULERS_PER_SM * sm_mhz * 1e6
 
     def add(stage, workload, ms, bytes_):
         gbs = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
         ncu = [{k: v for k, v in c.items() if k not in ("stage", "workload")} for c in counters
                if c.get("stage") == stage and c.get("workload") == workload]
         binding = None
+        issue = None
         if ncu:
             top = max(ncu, key=lambda c: c.get("duration_us") or 0)
             binding = top.get("binding")
+            instr = sum(c.get("warp_instructions") or 0 for c in ncu)
+            if instr > 0 and ms > 0:
+                min_ms = instr / issue_rate * 1e3
+                issue = {"warp_instructions": int(instr), "min_ms": round(min_ms, 4),
+                         "frac": round(min_ms / ms, 3), "sm_mhz": sm_mhz}
         rows.append({"stage": stage, "workload": workload, "ms": round(ms, 4), "algorithmic_bytes": int(bytes_),
                      "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak if gbs else None, "binding": binding,
-                     "ncu": ncu})
+                     "issue_roofline": issue, "ncu": ncu})
 
     c = line.get("counts", {})
     st = line.get("stages_ms", {})
@@ -1134,7 +1149,9 @@ def main():
         srv = line.get("serving", {}).get("1080p_1M")
         if srv and srv["best_served_at_p99_le_20ms"]:   # served frames against the drop-in C ABI per call
             srv["served_over_capi_per_call"] = srv["best_served_at_p99_le_20ms"]["served_frames_per_s"] / e2e["value"]
-    line["kernels"] = kernels_table(line, hbm_peak)
+    # the issue bound at the SM clock sampled during the timed frames
+    sm_mhz = (line.get("clocks") or {}).get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))
+    line["kernels"] = kernels_table(line, hbm_peak, float(sm_mhz))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if pg:
