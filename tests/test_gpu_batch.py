@@ -158,6 +158,25 @@ def test_interleaved_scene_groups(term_mode):
     check_views_against_single(views, RenderOptions(term_mode=term_mode))
 
 
+@pytest.mark.parametrize("term_mode", [0, 1])
+def test_distinct_scenes_with_empty_culled_and_ragged_views(term_mode):
+    """No two views share a scene, so every projection unit is one view's
+    block and the offset scan runs over the blocks of all views in turn:
+    views with no Gaussians, with every splat culled and with ragged block
+    counts between them, each equal to its standalone render."""
+    from lumen_b200 import render as R
+    empty = R.Scene(*(torch.zeros((0, k), device="cuda") for k in (3, 3, 4)), torch.zeros(0, device="cuda"),
+                    torch.zeros((0, 48), device="cuda"))
+    big = device_scene(scenes.box_scene(41_003, seed=41))
+    behind = device_scene(scenes.box_scene(700, seed=42, centre=(0, 0, -8)))
+    small = device_scene(scenes.box_scene(129, seed=43))
+    mid = device_scene(scenes.box_scene(9_871, seed=44, centre=(0, 0, 4)))
+    cams = scenes.orbit_cameras(5, 200, 136, radius=9.0)
+    views = [(big, cams[0]), (empty, cams[1]), (behind, cams[2]), (small, cams[3]), (mid, cams[4])]
+    b = check_views_against_single(views, RenderOptions(term_mode=term_mode))
+    assert float(b.images[2].rgb.abs().max()) == 0.0
+
+
 def test_same_scene_storage_with_different_counts_is_not_grouped():
     """Two scenes sharing parameter storage but with different Gaussian
     counts (a prefix of the arrays) are different groups: each view equals
