@@ -348,8 +348,8 @@ __device__ __forceinline__ bool intersect(const float4& a, const float4& b, cons
 
 struct CastArgs {
     const LumenBvhNode* nodes;
-    const int* splat_index;
-    long long node_count, root, n_gauss;
+    const int* splat_index;   /* n_leaves entries */
+    long long node_count, root, n_gauss, n_leaves;
     const float* means;
     const float* scales;
     float max_dist;
@@ -386,7 +386,9 @@ __device__ LumenRayHit cast_ray(const CastArgs& A, const float origin[3], const 
         if (!intersect(a, b, r, 0.0f, best.distance)) continue;
         const int left = __float_as_int(a.w), right = __float_as_int(b.w);
         if (left == -1 && right == -1) {
-            const int s = A.splat_index[idx];
+            /* leaves are nodes [0, n_leaves) of a built hierarchy; a damaged
+             * one cannot make the read leave the array */
+            const int s = (long long)idx < A.n_leaves ? A.splat_index[idx] : -1;
             if (s >= 0 && (long long)s < A.n_gauss) {
                 const float cx = A.means[(long long)s * 3], cy = A.means[(long long)s * 3 + 1],
                             cz = A.means[(long long)s * 3 + 2];
@@ -546,8 +548,8 @@ LumenStatus lumen_gpu_raycast(const LumenGpuBvh* bvh, const LumenGpuGaussians* g
     if (!bvh_ok(bvh, g) || n_rays < 0) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (n_rays == 0) return LUMEN_SUCCESS;
     if (!rays || !hits) return LUMEN_ERROR_INVALID_ARGUMENT;
-    const CastArgs A{bvh->nodes, bvh->splat_index, bvh->node_count, bvh->root_index, g->count, g->means,
-                     g->scales, max_dist};
+    const CastArgs A{bvh->nodes, bvh->splat_index, bvh->node_count, bvh->root_index, g->count, bvh->leaf_count,
+                     g->means, g->scales, max_dist};
     raycast_kernel<<<ray_grid(n_rays), 128, 0, (cudaStream_t)stream>>>(A, rays, n_rays, hits);
     return map_cuda(cudaGetLastError());
 }
@@ -558,8 +560,8 @@ LumenStatus lumen_gpu_pick_pixels(const LumenGpuBvh* bvh, const LumenGpuGaussian
     if (!bvh_ok(bvh, g) || !cam || n < 0) return LUMEN_ERROR_INVALID_ARGUMENT;
     if (n == 0) return LUMEN_SUCCESS;
     if (!pixels_xy || !hits) return LUMEN_ERROR_INVALID_ARGUMENT;
-    const CastArgs A{bvh->nodes, bvh->splat_index, bvh->node_count, bvh->root_index, g->count, g->means,
-                     g->scales, max_dist};
+    const CastArgs A{bvh->nodes, bvh->splat_index, bvh->node_count, bvh->root_index, g->count, bvh->leaf_count,
+                     g->means, g->scales, max_dist};
     pick_kernel<<<ray_grid(n), 128, 0, (cudaStream_t)stream>>>(A, *cam, pixels_xy, n, rays, hits);
     return map_cuda(cudaGetLastError());
 }
