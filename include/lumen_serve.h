@@ -10,7 +10,10 @@
  *  - requests queue in arrival order; a scheduler thread admits them into a
  *    batch while the batch fits a slot's work buffers (projection slots,
  *    tiles, an instance estimate learned per scene and resolution, output
- *    pixels) and max_views_per_batch;
+ *    pixels) and max_views_per_batch, and while its tiles number at most
+ *    65 536 (unless one view alone has more): batch-wide tile ids then sort
+ *    in two digit passes, where one tile more would add a third pass over
+ *    every instance of the batch;
  *  - up to max_batches_in_flight batches are on the device at once, each on
  *    its own stream with its own buffers, so a batch admitted while others
  *    run overlaps with them; a slot is reused as soon as its batch is done;

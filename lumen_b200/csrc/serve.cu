@@ -56,6 +56,13 @@ int variant_of(int chunk, int items) {
     return -1;
 }
 
+/* Tiles a batch holds unless one view alone has more: batch-wide tile ids
+ * below 2^16 sort in two 8-bit digit passes, and one tile more adds a third
+ * pass over every instance of the batch. That pass costs more per view than
+ * the further views share (1080p views of a 1M-Gaussian scene: 0.325 ms per
+ * view in a batch of 8, 65 280 tiles; 0.364 ms in a batch of 9). */
+constexpr int64_t kBatchTileIds = 1ll << 16;
+
 /* FIFO admission: the longest prefix of the queue whose sums fit. */
 int admit_prefix(const int64_t* slots, const int64_t* tiles, const int64_t* inst, const int64_t* pix, int n,
                  int max_views, int64_t max_slots, int64_t max_tiles, int64_t max_inst, int64_t max_pix) {
@@ -370,7 +377,11 @@ void scheduler_main(LumenServer* srv) {
             sl[i] = r.slots; ti[i] = r.tiles; in[i] = r.inst_est; px[i] = r.pixels;
         }
         int k = admit_prefix(sl.data(), ti.data(), in.data(), px.data(), n, srv->cfg.max_views_per_batch,
-                             srv->max_slots, srv->max_tiles, srv->max_inst, srv->max_pix);
+                             srv->max_slots, std::min<int64_t>(srv->max_tiles, kBatchTileIds), srv->max_inst,
+                             srv->max_pix);
+        if (k == 0 && ti[0] > kBatchTileIds)   /* a view of more tiles than that goes alone */
+            k = admit_prefix(sl.data(), ti.data(), in.data(), px.data(), 1, 1, srv->max_slots, srv->max_tiles,
+                             srv->max_inst, srv->max_pix);
         if (k == 0) {
             /* the front request does not fit with its margin: run it alone if
              * what it is known to need fits (an overflow raises the figure) */
