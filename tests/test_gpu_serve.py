@@ -196,3 +196,29 @@ def test_frozen_tuning_explores_nothing_and_images_unchanged(world):
         for r, ref in zip(out, refs):
             assert r.status == 0 and torch.equal(r.image, ref)
         srv.freeze_tuning(False)
+
+
+def test_batches_hold_at_most_65536_tiles():
+    """Admission stops before a batch's tiles pass 65 536 (batch-wide tile
+    ids of 16 bits, two tile-sort passes): 1080p views (8160 tiles) go at
+    most eight to a batch even when more are queued and max_views_per_batch
+    allows more; a view of more tiles than that is rendered alone. Every
+    image equals its standalone render."""
+    from lumen_b200 import serve
+    ds = device_scene(scenes.box_scene(3000, seed=52))
+    cams = scenes.orbit_cameras(20, 1920, 1080, radius=9.0)
+    wide = ViewCamera.from_fov(4200, 4200, 50.0)          # 263 x 263 = 69 169 tiles
+    with serve.Server(work_budget_bytes=4 << 30, max_views_per_batch=64, max_batches_in_flight=1,
+                      autotune=False) as srv:
+        st = srv.stats()
+        assert st["max_tiles"] >= 263 * 263 and st["max_pixels"] >= 4200 * 4200
+        sid = srv.add_scene(ds)
+        hs = [srv.submit(sid, c) for c in cams]
+        res = [h.result(timeout_ms=60_000) for h in hs]
+        w = srv.submit(sid, wide).result(timeout_ms=60_000)
+    views = [r.batch_views for r in res]
+    assert all(r.status == 0 for r in res) and max(views) <= 8 and max(views) >= 2, views
+    for i in (0, 7, 19):
+        assert torch.equal(res[i].image, alone_u8(ds, cams[i]))
+    assert w.status == 0 and w.batch_views == 1
+    assert torch.equal(w.image, alone_u8(ds, wide))
