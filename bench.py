@@ -428,7 +428,7 @@ def fwd_bwd_leg(dev, steps, warmup, hbm_peak):
         A.l1_loss(r, target).backward()
     torch.cuda.synchronize(dev)
     api_ms = (time.perf_counter() - t0) * 1e3 / ta_steps
-    b_fwd = 244 * n + 64 * V + (68 + 24 * passes) * K + 8 * T + 16 * P
+    b_fwd = 244 * n + 64 * V + (60 + 24 * passes) * K + 16 * T + 16 * P
     b_bwd = 80 * K + 12 * P + 88 * V + 472 * n
     total = b_fwd + 24 * P + b_bwd
     stages = {"project": fst[0] / reps, "sort": fst[1] / reps, "tile_ranges": fst[2] / reps,
@@ -682,7 +682,7 @@ def multiview_leg(dev, steps, warmup, hbm_peak):
     depth_keys = [r.varying_digits >> 8 for r in singles]
     depth_bytes = bin(int(np.bitwise_or.reduce(np.array(depth_keys))) & 0xFF).count("1")
     p = (tile_bits + 7) // 8 + depth_bytes
-    b = 236 * n + 8 * n * n_views + 64 * V + (68 + 24 * p) * K + 8 * T + 16 * P
+    b = 236 * n + 8 * n * n_views + 64 * V + (60 + 24 * p) * K + 16 * T + 16 * P
     return {"workload": "config 2: 300k Gaussians, 64 orbit views at 1280x720, one batch per step",
             "views_per_s": n_views * 1000.0 / ms, "ms_per_batch": ms,
             "per_call_views_per_s": n_views * 1000.0 / ms_single, "per_call_ms_for_64": ms_single,
@@ -983,16 +983,16 @@ def kernels_table(line, hbm_peak, sm_mhz=1965.0):
     P = WIDTH * HEIGHT
     if st:
         add("project", "config 1", st["project"], 236 * N + 48 * V + 4 * N)
-        add("sort", "config 1", st["sort"], 8 * N + 16 * V + 12 * K + 8 * K + 24 * K * p)
-        add("tile_ranges", "config 1", st["tile_ranges"], 8 * K + 8 * T)
+        add("sort", "config 1", st["sort"], 8 * N + 16 * V + 12 * K + 8 * K + 24 * K * p + 8 * T)
+        add("tile_ranges", "config 1", st["tile_ranges"], 8 * T)
         add("composite", "config 1", st["composite"], 40 * K + 16 * P)
     fb = line.get("fwd_bwd")
     if fb and "stages_ms" in fb:
         z, s3 = fb["sizes"], fb["stages_ms"]
         n3, V3, K3, P3, T3, p3 = z["n"], z["visible"], z["instances"], z["pixels"], z["tiles"], z["digit_passes"]
         add("project", "config 3", s3["project"], 236 * n3 + 48 * V3 + 4 * n3)
-        add("sort", "config 3", s3["sort"], 8 * n3 + 16 * V3 + 12 * K3 + 8 * K3 + 24 * K3 * p3)
-        add("tile_ranges", "config 3", s3["tile_ranges"], 8 * K3 + 8 * T3)
+        add("sort", "config 3", s3["sort"], 8 * n3 + 16 * V3 + 12 * K3 + 8 * K3 + 24 * K3 * p3 + 8 * T3)
+        add("tile_ranges", "config 3", s3["tile_ranges"], 8 * T3)
         add("composite", "config 3", s3["composite"], 40 * K3 + 16 * P3)
         add("composite_backward", "config 3", s3["composite_backward"], 80 * K3 + 12 * P3)
         add("project_backward", "config 3", s3["project_backward"], 88 * V3 + 472 * n3)
@@ -1102,8 +1102,8 @@ def main():
     P = WIDTH * HEIGHT
     p = passes
     alg = {"project": 236 * N_GAUSSIANS + 48 * V + 4 * N_GAUSSIANS,
-           "sort": 8 * N_GAUSSIANS + 16 * V + 12 * K + 8 * K + 24 * K * p,
-           "tile_ranges": 8 * K + 8 * T,
+           "sort": 8 * N_GAUSSIANS + 16 * V + 12 * K + 8 * K + 24 * K * p + 8 * T,
+           "tile_ranges": 8 * T,
            "composite": 40 * K + 16 * P}
     # the dominant kernel: composite_kernel, the largest share of the frame's
     # launch list (profiles/forward_config1_launches.md); the sort stage is
@@ -1111,7 +1111,7 @@ def main():
     dom = names.index("composite")
     dname = names[dom]
     achieved = alg[dname] / (stage_ms[dom] * 1e-3) / 1e9
-    b_fwd = 244 * N_GAUSSIANS + 64 * V + (68 + 24 * passes) * K + 8 * T + 16 * P
+    b_fwd = 244 * N_GAUSSIANS + 64 * V + (60 + 24 * passes) * K + 16 * T + 16 * P
     frame_gbs = b_fwd / (ms_max * 1e-3) / 1e9
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,

@@ -39,8 +39,8 @@ void launch_emit(const ViewTable* vt, const LumenGpuFrame& f, Control* ctrl, uns
                  unsigned int* sort_lb, long long sort_lb_tiles, int sort_tile_keys, long long n_blocks,
                  bool persistent, int num_sms, cudaStream_t st);
 void launch_tile_sort_counted(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1,
-                              long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap,
-                              unsigned int* err, int items, int key_bytes, int num_sms, cudaStream_t st);
+                              long long capacity, Control* ctrl, ViewTable* vt, int* ranges, unsigned int* lb,
+                              long long lb_tiles_cap, int items, int key_bytes, int num_sms, cudaStream_t st);
 void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1, long long capacity,
                    SortControl* sc, unsigned int* lb, long long lb_tiles_cap, int* ranges,
                    const long long* n_range_tiles, unsigned int* err, int items, int key_bytes, int num_sms,
@@ -212,9 +212,8 @@ void launch_pipeline(const ScratchLayout& L, unsigned char* base, const LumenRen
     int tile_bytes = 0;
     for (long long t = n_tiles - 1; t > 0; t >>= 8) ++tile_bytes;
     if (n_slots > 0)
-        launch_tile_sort_counted(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort,
-                                 tile_lb, 2 * L.sort_tiles, &ctrl->error_flags, lc.tile_sort_items, tile_bytes, sms,
-                                 s);
+        launch_tile_sort_counted(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, ctrl, vt,
+                                 f.ranges, tile_lb, 2 * L.sort_tiles, lc.tile_sort_items, tile_bytes, sms, s);
     else
         launch_sort32(f.keys[0], f.vals[0], f.keys[1], f.vals[1], f.instance_capacity, &ctrl->tile_sort, tile_lb,
                       2 * L.sort_tiles, f.ranges, &vt->hdr.total_tiles, &ctrl->error_flags, lc.tile_sort_items,

@@ -23,6 +23,12 @@
  *    written out in digit runs.
  *  - every wait on another CTA's descriptor is bounded.
  * Per pass and pair: (sizeof key + 4) B read and written.
+ *
+ * Tile ranges: the frame's tile sort leaves its ids in final order in the
+ * pass over the highest varying byte, which writes each tile's range from
+ * the edges of the runs of equal ids in its pass tiles (atomic minimum of
+ * the run starts, maximum of the run ends); a small kernel then counts the
+ * touched tiles and finds each view's first instance from the ranges.
  */
 #include "splat_common.cuh"
 
@@ -185,11 +191,41 @@ __device__ __forceinline__ unsigned int lookback_digit(const unsigned int* lb, i
     return excl;
 }
 
+/* Where the tile sort's last digit pass writes the tile ranges
+ * (binning.mojo:51-73), or ranges == nullptr for every other sort. The
+ * ranges hold (-1, -1) before the sort. */
+struct TileRangeSink {
+    int* ranges;
+    const long long* n_tiles;   /* the batch's tile count (ids at or above it are a bounds error) */
+    unsigned int* done;         /* set to 1 by the pass that wrote the ranges */
+};
+
+/* Key j of a pass tile (nvalid keys, in sorted order in shared memory) went
+ * to global position pos. A digit's keys go to consecutive positions, so a
+ * run of equal ids inside the pass tile covers consecutive positions: the
+ * tile's range starts at the smallest run start over all pass tiles and ends
+ * after the largest run end (a range's -1 start is the largest unsigned
+ * value, so the minimum replaces it). */
+template <typename KeyT>
+__device__ __forceinline__ void tile_range_edges(const TileRangeSink& sink, const KeyT* skeys, int j, int nvalid,
+                                                 KeyT kk, long long pos, long long n_tiles, unsigned int* err) {
+    const bool first = j == 0 || skeys[j - 1] != kk;
+    const bool last = j + 1 == nvalid || skeys[j + 1] != kk;
+    if (!first && !last) return;
+    const unsigned int t = (unsigned int)kk;
+    if ((long long)t >= n_tiles) {   /* self-check: a tile id outside the grid */
+        atomicOr(err, LUMEN_GPU_ERR_BOUNDS);
+        return;
+    }
+    if (first) atomicMin(reinterpret_cast<unsigned int*>(sink.ranges + 2 * (size_t)t), (unsigned int)pos);
+    if (last) atomicMax(sink.ranges + 2 * (size_t)t + 1, (int)(pos + 1));
+}
+
 /* kItems keys per thread: tiles of 256 * kItems keys. */
 template <typename KeyT, int kItems>
 __global__ void __launch_bounds__(kSortThreads, sizeof(KeyT) == 4 ? (kItems <= 8 ? 4 : kItems <= 16 ? 3 : 2) : 2)
 onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
-                     unsigned int* lb_all, long long lb_tiles_cap, unsigned int* err, int digit) {
+                     unsigned int* lb_all, long long lb_tiles_cap, unsigned int* err, int digit, TileRangeSink sink) {
     chain_begin();
     constexpr int kTileKeys = kSortThreads * kItems;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -213,6 +249,12 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
     const long long ntiles = (K + kTileKeys - 1) / kTileKeys;
     const int shift = 8 * digit;
     unsigned int* lb = lb_all + (size_t)digit * (size_t)lb_tiles_cap * 256;
+    /* the pass over the highest varying digit leaves the ids in their final
+     * order and writes the tile ranges from the run edges it sees in each
+     * pass tile (32-bit tile ids only) */
+    const bool emit_ranges = sizeof(KeyT) == 4 && sink.ranges != nullptr && (varying >> digit) == 1u;
+    const long long n_tiles = emit_ranges ? *sink.n_tiles : 0;
+    if (emit_ranges && blockIdx.x == 0 && tid == 0) *sink.done = 1u;
 
     /* global exclusive offsets of this digit's buckets */
     {
@@ -339,6 +381,7 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
                 const long long out = s.gbase[d] + j;
                 kout[out] = kk;
                 vout[out] = s.vals[j];
+                if (emit_ranges) tile_range_edges(sink, s.keys, j, kTileKeys, kk, out, n_tiles, err);
             }
         } else {
             for (int j = tid; j < nvalid; j += kSortThreads) {
@@ -347,15 +390,47 @@ onesweep_pass_kernel(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lon
                 const long long out = s.gbase[d] + j;
                 kout[out] = kk;
                 vout[out] = s.vals[j];
+                if (emit_ranges) tile_range_edges(sink, s.keys, j, nvalid, kk, out, n_tiles, err);
             }
         }
         __syncthreads();
     }
 }
 
+/* When the tile sort's last digit pass wrote the ranges: the touched-tile
+ * count and each view's first instance (the smallest range start among its
+ * tiles; tile ids are view-major), from the 2 * n_tiles range entries. */
+__device__ void ranges_epilogue(ViewTable* vt, const int* ranges, Control* ctrl) {
+    const long long n_tiles = vt->hdr.total_tiles;
+    const int n_views = vt->hdr.n_views;
+    const int lane = threadIdx.x & 31;
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    unsigned int touched = 0;
+    for (long long wb = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n_tiles; wb += nthreads) {
+        const long long t = wb + lane;
+        const bool valid = t < n_tiles;
+        /* an empty tile's start, -1, is the largest unsigned value */
+        const unsigned int start = valid ? (unsigned int)ranges[2 * (size_t)t] : 0xFFFFFFFFu;
+        touched += start != 0xFFFFFFFFu;
+        const int v = !valid ? -1 : n_views > 1 ? find_view_by_tile(vt, n_views, t) : 0;
+        const int v0 = __shfl_sync(0xffffffffu, v, 0);
+        if (__all_sync(0xffffffffu, v == v0 || v < 0)) {
+            const unsigned int m = __reduce_min_sync(0xffffffffu, start);
+            if (lane == 0 && m != 0xFFFFFFFFu)
+                atomicMin(reinterpret_cast<unsigned long long*>(&vt->view[v0].inst_begin), (unsigned long long)m);
+        } else if (start != 0xFFFFFFFFu) {
+            atomicMin(reinterpret_cast<unsigned long long*>(&vt->view[v].inst_begin), (unsigned long long)start);
+        }
+    }
+    touched = __reduce_add_sync(0xffffffffu, touched);
+    if (lane == 0 && touched) atomicAdd(&ctrl->touched_tiles, touched);
+}
+
 /* binning.mojo:51-73 in parallel, on tile-sorted 32-bit tile ids: a tile's
  * range starts where its id first appears and ends after it last appears.
- * Empty tiles keep the (-1, -1) written before the sort.
+ * Empty tiles keep the (-1, -1) written before the sort. When a tile-id byte
+ * varies, the tile sort's last digit pass has written the ranges and this
+ * kernel only finishes them (ranges_epilogue); otherwise it reads the ids:
  *
  * Each lane takes 8 consecutive ids per round (two 16-byte loads; the
  * frame's key buffers are 16-byte aligned) and its neighbours' ids come
@@ -368,6 +443,10 @@ __global__ void __launch_bounds__(256)
 tile_ranges_kernel(const unsigned int* k0, const unsigned int* k1, long long capacity, ViewTable* vt,
                    int* ranges, Control* ctrl) {
     chain_begin();
+    if (ctrl->ranges_by_sort) {
+        ranges_epilogue(vt, ranges, ctrl);
+        return;
+    }
     const SortControl* sc = &ctrl->tile_sort;
     const long long n_tiles = vt->hdr.total_tiles;
     const int n_views = vt->hdr.n_views;
@@ -468,7 +547,8 @@ __global__ void sorted_keys64_kernel(const unsigned int* k0, const unsigned int*
 template <typename KeyT, int kItems>
 void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, long long capacity, SortControl* sc,
                       unsigned int* lb, long long lb_tiles_cap, int* ranges, const long long* n_range_tiles,
-                      unsigned int* err, int key_bytes, int num_sms, cudaStream_t st, bool counted = false) {
+                      unsigned int* err, int key_bytes, int num_sms, cudaStream_t st, bool counted = false,
+                      TileRangeSink sink = TileRangeSink{}) {
     if (!counted)
         launch_chained(histogram_kernel<KeyT>, dim3(num_sms * 4), dim3(256), 0, st, (const KeyT*)k0, capacity, sc, lb,
                        lb_tiles_cap, kSortThreads * kItems, ranges, n_range_tiles);
@@ -478,7 +558,7 @@ void launch_sort_impl(KeyT* k0, unsigned int* v0, KeyT* k1, unsigned int* v1, lo
     const int nd = key_bytes < (int)sizeof(KeyT) ? key_bytes : (int)sizeof(KeyT);
     for (int d = 0; d < nd; ++d)
         launch_chained(onesweep_pass_kernel<KeyT, kItems>, dim3(num_sms * ctas_per_sm), dim3(kSortThreads), smem, st,
-                       k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d);
+                       k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, err, d, sink);
 }
 
 /* items: keys per thread of a digit pass, 8, 16 or 24 (tiles of 2048, 4096
@@ -500,20 +580,23 @@ void launch_sort32(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigne
 }
 
 /* The frame's tile sort when the emission has counted the digit values,
- * cleared the look-back tiles and filled the ranges: the digit passes
- * only. */
+ * cleared the look-back tiles and filled the ranges with -1: the digit
+ * passes only, the last of which writes the tile ranges. */
 void launch_tile_sort_counted(unsigned int* k0, unsigned int* v0, unsigned int* k1, unsigned int* v1,
-                              long long capacity, SortControl* sc, unsigned int* lb, long long lb_tiles_cap,
-                              unsigned int* err, int items, int key_bytes, int num_sms, cudaStream_t st) {
+                              long long capacity, Control* ctrl, ViewTable* vt, int* ranges, unsigned int* lb,
+                              long long lb_tiles_cap, int items, int key_bytes, int num_sms, cudaStream_t st) {
+    SortControl* sc = &ctrl->tile_sort;
+    unsigned int* err = &ctrl->error_flags;
+    const TileRangeSink sink{ranges, &vt->hdr.total_tiles, &ctrl->ranges_by_sort};
     if (items == 8)
         launch_sort_impl<unsigned int, 8>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
-                                          key_bytes, num_sms, st, true);
+                                          key_bytes, num_sms, st, true, sink);
     else if (items == 24)
         launch_sort_impl<unsigned int, 24>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
-                                           key_bytes, num_sms, st, true);
+                                           key_bytes, num_sms, st, true, sink);
     else
         launch_sort_impl<unsigned int, 16>(k0, v0, k1, v1, capacity, sc, lb, lb_tiles_cap, nullptr, nullptr, err,
-                                           key_bytes, num_sms, st, true);
+                                           key_bytes, num_sms, st, true, sink);
 }
 
 void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long* k1, unsigned int* v1,
@@ -524,11 +607,11 @@ void launch_sort64(unsigned long long* k0, unsigned int* v0, unsigned long long*
 }
 
 void launch_ranges(const LumenGpuFrame& f, Control* ctrl, ViewTable* vt, int num_sms, cudaStream_t st) {
-    /* about one group of 8 ids per thread at full capacity (the loads are
-     * independent, so more threads in flight hide their latency) */
-    long long grid = ((long long)f.instance_capacity + 256 * kRangeIds - 1) / (256 * kRangeIds);
-    if (grid < num_sms * 4) grid = num_sms * 4;
-    if (grid > (1ll << 20)) grid = 1ll << 20;
+    /* the tile sort's last digit pass writes the ranges whenever a tile-id
+     * byte varies, and this launch then reads only the ranges (2 * n_tiles
+     * ints); otherwise (every id equal, or none) the ids are one run, which
+     * a grid-stride loop over num_sms * 2 CTAs reads in a few rounds */
+    const long long grid = (long long)num_sms * 2;
     launch_chained(tile_ranges_kernel, dim3((unsigned int)grid), dim3(256), 0, st, (const unsigned int*)f.keys[0],
                    (const unsigned int*)f.keys[1], (long long)f.instance_capacity, vt, f.ranges, ctrl);
 }

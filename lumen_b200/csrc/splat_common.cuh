@@ -52,7 +52,8 @@ struct Control {
     unsigned int composite_ticket;       /* tile order of the compositor */
     unsigned int count_ticket;           /* unit order of the batch visibility count */
     unsigned int offsets_ticket;         /* tile order of the batch offset scan */
-    unsigned int pad[6];
+    unsigned int ranges_by_sort;         /* 1: the tile sort's last digit pass wrote the tile ranges */
+    unsigned int pad[5];
     SortControl depth_sort;              /* visible splats by depth key */
     SortControl tile_sort;               /* instances by tile id */
 };
