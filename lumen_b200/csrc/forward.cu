@@ -13,8 +13,10 @@
  *   emit               K2: (tile id, visible index) per covered tile, in depth order;
  *                      also the tile sort's digit counts, look-back tiles and ranges = -1
  *   onesweep_pass xb   stable sort of instances by tile id (b: the bytes a tile id
- *                      can vary in; with no Gaussians a histogram launch comes first)
- *   tile_ranges        K4
+ *                      can vary in; with no Gaussians a histogram launch comes first);
+ *                      the pass over the highest varying byte writes the tile ranges
+ *   tile_ranges        K4: touched tiles and each view's first instance from the
+ *                      ranges (the ranges themselves when no tile-id byte varies)
  *   composite          K5
  * Passes whose digit is constant exit at once (decided on the device).
  */
