@@ -138,6 +138,26 @@ def test_empty_and_fully_culled():
     assert_parity(g, o)
 
 
+def test_every_instance_in_one_tile_of_many():
+    """Small splats stacked over one tile of a 4x4-tile frame: every tile id
+    is equal, so no digit pass reorders anything and the ranges come from
+    the sorted ids (the tile sort's last pass writes them only when a
+    tile-id byte varies); then a frame of a single instance."""
+    cam = ViewCamera((0, 0, 0), (1, 0, 0, 0), 50, 50, 32, 32, 0.1, 100, 64, 64)
+    n = 5
+    z = 4.0 + 0.5 * np.arange(n, dtype=np.float32)
+    means = np.stack([(24.0 - 32.0) / 50 * z, (40.0 - 32.0) / 50 * z, z], 1).astype(np.float32)
+    scales = np.full((n, 3), 0.001, np.float32)
+    quats = np.tile(np.array([1, 0, 0, 0], np.float32), (n, 1))
+    op = np.full(n, 0.6, np.float32)
+    sh = np.zeros((n, 48), np.float32)
+    sh[:, 0] = 1.0
+    for m in (n, 1):
+        g, o = run_both(means[:m], scales[:m], quats[:m], op[:m], sh[:m], cam, RenderOptions())
+        assert o.n_instances == m and np.unique(o.keys_sorted >> np.uint64(32)).size == 1
+        assert_parity(g, o, check_image_bits=True)
+
+
 def test_degenerate_parameters():
     # zero scales (tests/test_regressions.mojo:26-57), unnormalised and zero quaternions,
     # transparent splats, splats on the near plane
